@@ -1,0 +1,380 @@
+"""TEST INFRASTRUCTURE -- numpy wrappers over the CPU oracle.
+
+``C``   : liboracle.so, the plain-C restatement (pc_oracle.c).
+``REF`` : _ref/libpcref.so, the reference's own Graph.cpp with a C entry layer
+          (ref_capi.cpp), present when it was built (see Makefile).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle.so"
+REF_SO = HERE / "_ref" / "libpcref.so"
+REF_SRC = Path(os.environ.get("PC_REFERENCE_DIR", "/root/reference"))
+
+P = C.c_void_p
+i32, u64, f32, f64 = C.c_int32, C.c_uint64, C.c_float, C.c_double
+
+
+def build(ref: bool = True):
+    """Builds liboracle.so, and the reference library when its sources exist."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True)
+    if ref and (REF_SRC / "src" / "Graph.cpp").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={REF_SRC}"], check=True)
+
+
+def _ptr(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _load_c():
+    if not ORACLE_SO.exists():
+        build(ref=False)
+    lib = C.CDLL(str(ORACLE_SO))
+    sig = {
+        "or_tc_merge": (u64, [u64, P, P]),
+        "or_tc_galloping": (u64, [u64, P, P]),
+        "or_layout": (C.c_int, [u64, P, P, P, P, i32, P, P, P]),
+        "or_tc_partitioned": (u64, [u64, P, P, i32]),
+        "or_lcc": (None, [u64, P, P, P]),
+        "or_jaccard_edges": (None, [u64, P, P, P]),
+        "or_jaccard_queries": (None, [u64, P, P, P, i32, P]),
+        "or_batch_pairs": (None, [u64, P, P, P, u64, P]),
+        "or_batch_sets": (None, [u64, P, P, P, P, u64, P]),
+        "or_bfs": (None, [u64, P, P, i32, P]),
+        "or_sssp": (None, [u64, P, P, P, i32, P]),
+        "or_pagerank_f64": (None, [u64, P, P, f64, i32, P, P]),
+        "or_kcore": (i32, [u64, P, P, P]),
+        "or_mis": (None, [u64, P, P, P]),
+        "or_mis_priority": (None, [u64, P, P, P, P]),
+        "or_cdlp": (None, [u64, P, P, i32, P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+_C = None
+
+
+def clib():
+    global _C
+    if _C is None:
+        _C = _load_c()
+    return _C
+
+
+def _csr(vl, el):
+    vl = np.ascontiguousarray(vl, np.uint64)
+    el = np.ascontiguousarray(el, np.int32)
+    return vl, el, vl.size - 1
+
+
+# ---- the C restatement ---------------------------------------------------------
+
+def tc_merge(vl, el):
+    vl, el, n = _csr(vl, el)
+    return int(clib().or_tc_merge(n, _ptr(vl), _ptr(el)))
+
+
+def tc_galloping(vl, el):
+    vl, el, n = _csr(vl, el)
+    return int(clib().or_tc_galloping(n, _ptr(vl), _ptr(el)))
+
+
+def layout(vl, el, w, v2p):
+    vl, el, n = _csr(vl, el)
+    v2p = np.ascontiguousarray(v2p, np.int32)
+    P_ = int(v2p.max()) + 1 if n else 1
+    ovl = np.empty(P_ * n + 1, np.uint64)
+    oel = np.empty(el.size, np.int32)
+    ow = None if w is None else np.empty(el.size, np.int32)
+    wa = None if w is None else np.ascontiguousarray(w, np.int32)
+    clib().or_layout(n, _ptr(vl), _ptr(el), _ptr(wa), _ptr(v2p), P_, _ptr(ovl), _ptr(oel), _ptr(ow))
+    return ovl, oel, ow
+
+
+def tc_partitioned(pvl, pel, n, P_):
+    pvl = np.ascontiguousarray(pvl, np.uint64)
+    pel = np.ascontiguousarray(pel, np.int32)
+    return int(clib().or_tc_partitioned(n, _ptr(pvl), _ptr(pel), P_))
+
+
+def lcc(vl, el):
+    vl, el, n = _csr(vl, el)
+    out = np.empty(n, np.float64)
+    clib().or_lcc(n, _ptr(vl), _ptr(el), _ptr(out))
+    return out
+
+
+def jaccard_edges(vl, el):
+    vl, el, n = _csr(vl, el)
+    out = np.empty(el.size, np.float32)
+    clib().or_jaccard_edges(n, _ptr(vl), _ptr(el), _ptr(out))
+    return out
+
+
+def jaccard_queries(vl, el, q):
+    vl, el, n = _csr(vl, el)
+    q = np.ascontiguousarray(q, np.int32)
+    out = np.empty(q.size * q.size, np.float64)
+    clib().or_jaccard_queries(n, _ptr(vl), _ptr(el), _ptr(q), q.size, _ptr(out))
+    return out
+
+
+def batch_pairs(vl, el, pairs):
+    vl, el, n = _csr(vl, el)
+    pairs = np.ascontiguousarray(pairs, np.int32).reshape(-1)
+    out = np.empty(pairs.size // 2, np.uint64)
+    clib().or_batch_pairs(n, _ptr(vl), _ptr(el), _ptr(pairs), pairs.size // 2, _ptr(out))
+    return out
+
+
+def batch_sets(vl, el, sets):
+    vl, el, n = _csr(vl, el)
+    ids = np.concatenate([np.asarray(s, np.int32) for s in sets]) if sets else np.zeros(0, np.int32)
+    offs = np.zeros(len(sets) + 1, np.uint64)
+    np.cumsum([len(s) for s in sets], out=offs[1:])
+    out = np.empty(len(sets), np.uint64)
+    clib().or_batch_sets(n, _ptr(vl), _ptr(el), _ptr(ids), _ptr(offs), len(sets), _ptr(out))
+    return out
+
+
+def bfs(vl, el, src):
+    vl, el, n = _csr(vl, el)
+    out = np.empty(n, np.int32)
+    clib().or_bfs(n, _ptr(vl), _ptr(el), src, _ptr(out))
+    return out
+
+
+def sssp(vl, el, w, src):
+    vl, el, n = _csr(vl, el)
+    w = np.ascontiguousarray(w, np.int32)
+    out = np.empty(n, np.int32)
+    clib().or_sssp(n, _ptr(vl), _ptr(el), _ptr(w), src, _ptr(out))
+    return out
+
+
+def pagerank_f64(vl, el, damping=0.85, iters=20, init=None):
+    vl, el, n = _csr(vl, el)
+    out = np.empty(n, np.float64)
+    ini = None if init is None else np.ascontiguousarray(init, np.float64)
+    clib().or_pagerank_f64(n, _ptr(vl), _ptr(el), damping, iters, _ptr(ini), _ptr(out))
+    return out
+
+
+def kcore(vl, el):
+    vl, el, n = _csr(vl, el)
+    out = np.empty(n, np.int32)
+    largest = clib().or_kcore(n, _ptr(vl), _ptr(el), _ptr(out))
+    return out, int(largest)
+
+
+def mis(vl, el, priority=None):
+    vl, el, n = _csr(vl, el)
+    out = np.zeros(n, np.int32)
+    if priority is None:
+        clib().or_mis(n, _ptr(vl), _ptr(el), _ptr(out))
+    else:
+        pr = np.ascontiguousarray(priority, np.uint64)
+        clib().or_mis_priority(n, _ptr(vl), _ptr(el), _ptr(pr), _ptr(out))
+    return out
+
+
+def cdlp(vl, el, labels, iters=10):
+    vl, el, n = _csr(vl, el)
+    lab = np.ascontiguousarray(labels, np.int32).copy()
+    clib().or_cdlp(n, _ptr(vl), _ptr(el), iters, _ptr(lab))
+    return lab
+
+
+# ---- the reference itself (oracle/_ref) ------------------------------------------
+
+class Reference:
+    """The reference library (libpcref.so) on one graph, written to a temporary
+    CSR directory in the reference's binary format and loaded by its own
+    Graph(csrdir, is_weighted) constructor."""
+
+    _lib = None
+
+    @classmethod
+    def available(cls) -> bool:
+        return REF_SO.exists()
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            if not REF_SO.exists():
+                raise FileNotFoundError(f"{REF_SO} not built")
+            lib = C.CDLL(str(REF_SO))
+            sig = {
+                "ref_graph_load": (P, [C.c_char_p, C.c_int]),
+                "ref_graph_free": (None, [P]),
+                "ref_graph_n": (u64, [P]),
+                "ref_graph_m": (u64, [P]),
+                "ref_pgraph_new": (P, [P, P, u64, C.c_int]),
+                "ref_pgraph_free": (None, [P]),
+                "ref_pgraph_partitions": (u64, [P]),
+                "ref_pgraph_reorder": (None, [P]),
+                "ref_pgraph_layout": (None, [P, P, P, P]),
+                "ref_pgraph_evaluate": (None, [P]),
+                "ref_tc_graph": (u64, [P, C.c_int, C.c_int]),
+                "ref_tc_pgraph": (u64, [P, C.c_int]),
+                "ref_tc_rows": (u64, [P, P, u64, C.c_int]),
+                "ref_lcc_graph": (None, [P, C.c_int, C.c_int, P]),
+                "ref_lcc_pgraph": (None, [P, C.c_int, P]),
+                "ref_jsim_graph": (None, [P, P, i32, C.c_int, P]),
+                "ref_jsim_pgraph": (None, [P, P, i32, P]),
+                "ref_batch_pairs": (None, [P, C.c_int, P, u64, C.c_int, P]),
+                "ref_batch_sets": (None, [P, C.c_int, P, P, u64, C.c_int, P]),
+                "ref_bfs_graph": (None, [P, i32, P]),
+                "ref_sssp": (None, [P, C.c_int, u64, i32, P]),
+                "ref_pagerank": (None, [P, C.c_int, u64, f32, C.c_int, C.c_int, P]),
+                "ref_kcore": (None, [P, C.c_int, u64, C.c_int, P]),
+                "ref_mis": (None, [P, C.c_int, u64, C.c_int, P]),
+                "ref_cdlp": (None, [P, C.c_int, u64, C.c_int, C.c_int, P]),
+            }
+            for name, (res, args) in sig.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, vl, el, w=None, v2p=None, threads=None, csrdir=None):
+        lib = self.lib()
+        self.threads = threads or os.cpu_count() or 1
+        self._tmp = None
+        if csrdir is None:
+            self._tmp = tempfile.TemporaryDirectory(prefix="pcref_")
+            csrdir = self._tmp.name
+            np.ascontiguousarray(vl, np.uint64).tofile(os.path.join(csrdir, "csr_vlist.bin"))
+            np.ascontiguousarray(el, np.int32).tofile(os.path.join(csrdir, "csr_elist.bin"))
+            if w is not None:
+                np.ascontiguousarray(w, np.int32).tofile(os.path.join(csrdir, "csr_weight.bin"))
+        self.g = lib.ref_graph_load(csrdir.encode(), int(w is not None))
+        self.n = int(lib.ref_graph_n(self.g))
+        self.m = int(lib.ref_graph_m(self.g))
+        self.pg = None
+        if v2p is not None:
+            self.v2p = np.ascontiguousarray(v2p, np.int32)
+            self.pg = lib.ref_pgraph_new(self.g, _ptr(self.v2p), self.n, self.threads)
+
+    def close(self):
+        lib = self.lib()
+        if self.pg:
+            lib.ref_pgraph_free(self.pg)
+            self.pg = None
+        if self.g:
+            lib.ref_graph_free(self.g)
+            self.g = None
+        if self._tmp is not None:
+            self._tmp.cleanup()
+            self._tmp = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _obj(self, partitioned):
+        if partitioned and not self.pg:
+            raise ValueError("no partition given")
+        return self.pg if partitioned else self.g
+
+    def tc(self, partitioned=False, galloping=False):
+        lib = self.lib()
+        if partitioned:
+            return int(lib.ref_tc_pgraph(self.pg, int(galloping)))
+        return int(lib.ref_tc_graph(self.g, int(galloping), self.threads))
+
+    def tc_rows(self, rows):
+        r = np.ascontiguousarray(rows, np.int32)
+        return int(self.lib().ref_tc_rows(self.g, _ptr(r), r.size, self.threads))
+
+    def layout(self):
+        P_ = int(self.lib().ref_pgraph_partitions(self.pg))
+        vl = np.empty(P_ * self.n + 1, np.uint64)
+        el = np.empty(self.m, np.int32)
+        self.lib().ref_pgraph_layout(self.pg, _ptr(vl), _ptr(el), None)
+        return vl, el
+
+    def reorder(self):
+        self.lib().ref_pgraph_reorder(self.pg)
+
+    def lcc(self, partitioned=False, galloping=False):
+        out = np.empty(self.n, np.float64)
+        if partitioned:
+            self.lib().ref_lcc_pgraph(self.pg, int(galloping), _ptr(out))
+        else:
+            self.lib().ref_lcc_graph(self.g, int(galloping), self.threads, _ptr(out))
+        return out
+
+    def jsim(self, q, partitioned=False):
+        q = np.ascontiguousarray(q, np.int32)
+        out = np.empty(q.size * q.size, np.float64)
+        if partitioned:
+            self.lib().ref_jsim_pgraph(self.pg, _ptr(q), q.size, _ptr(out))
+        else:
+            self.lib().ref_jsim_graph(self.g, _ptr(q), q.size, self.threads, _ptr(out))
+        return out
+
+    def batch_pairs(self, pairs, partitioned=False):
+        p = np.ascontiguousarray(pairs, np.int32).reshape(-1)
+        out = np.empty(p.size // 2, np.uint64)
+        self.lib().ref_batch_pairs(self._obj(partitioned), int(partitioned), _ptr(p), p.size // 2, self.threads,
+                                   _ptr(out))
+        return out
+
+    def batch_sets(self, sets, partitioned=False):
+        ids = np.concatenate([np.asarray(s, np.int32) for s in sets])
+        offs = np.zeros(len(sets) + 1, np.uint64)
+        np.cumsum([len(s) for s in sets], out=offs[1:])
+        out = np.empty(len(sets), np.uint64)
+        self.lib().ref_batch_sets(self._obj(partitioned), int(partitioned), _ptr(ids), _ptr(offs), len(sets),
+                                  self.threads, _ptr(out))
+        return out
+
+    def bfs_parents(self, src):
+        out = np.empty(self.n, np.int32)
+        self.lib().ref_bfs_graph(self.g, src, _ptr(out))
+        return out
+
+    def sssp(self, src, partitioned=False):
+        out = np.empty(self.n, np.int32)
+        self.lib().ref_sssp(self._obj(partitioned), int(partitioned), self.n, src, _ptr(out))
+        return out
+
+    def pagerank(self, damping=0.85, iters=20, partitioned=True):
+        out = np.empty(self.n, np.float32)
+        self.lib().ref_pagerank(self._obj(partitioned), int(partitioned), self.n, damping, iters, self.threads,
+                                _ptr(out))
+        return out
+
+    def kcore(self, partitioned=False):
+        out = np.empty(self.n, np.int32)
+        self.lib().ref_kcore(self._obj(partitioned), int(partitioned), self.n, self.threads, _ptr(out))
+        return out
+
+    def mis(self, partitioned=False):
+        out = np.empty(self.n, np.int32)
+        self.lib().ref_mis(self._obj(partitioned), int(partitioned), self.n, self.threads, _ptr(out))
+        return out
+
+    def cdlp(self, labels, iters=10, partitioned=False):
+        lab = np.ascontiguousarray(labels, np.int32).copy()
+        self.lib().ref_cdlp(self._obj(partitioned), int(partitioned), self.n, iters, self.threads, _ptr(lab))
+        return lab

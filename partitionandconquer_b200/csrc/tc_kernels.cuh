@@ -1,0 +1,233 @@
+// Triangle-counting intersection kernels (sm_100a).
+//
+// Work decomposition ("pivot" form).  Orient every undirected edge from the
+// larger id to the smaller id; with degree-descending ids this is the degree
+// orientation.  Let N+(x) = N(x) & [0, x) -- the prefix of x's sorted row, of
+// length dplus[x] -- and N-(x) the suffix (ids > x).  A triangle a < b < c is
+// found exactly once, at pivot b and in-neighbour c in N-(b), as the element
+// a of N(c) & [0, b) that is also in N+(b).  Hence
+//     T = sum_b sum_{c in N-(b)} |N(c) & [0,b) & N+(b)|,
+// the same number as the reference's sum over partitions of
+// cnt_common_neis_less_than_merge(u, v, v, i) (src/Graph.cpp:1346-1362): both
+// count every triangle once.  Every kernel processes all in-edges of a set
+// of pivots, so kernels can be mixed per partition and the total stays exact.
+//
+// Work items are (pivot, chunk of in-neighbours) pairs taken from a global
+// counter, so hub pivots with 10^5 in-neighbours are spread over many CTAs.
+//
+// Pivot sets in shared memory:
+//  * bitmap (CTA-wide): bit a set for a in N+(b), needs b <= capacity;
+//  * hash (warp-private): open addressing, <= 256 keys in 512 slots;
+//  * none: threshold merge (the reference's primitive) or binary search.
+#pragma once
+#include <stdint.h>
+
+#include "pc_internal.cuh"
+
+namespace pc {
+namespace tc {
+
+constexpr int kTile = 16384;        // pivots per planning tile
+constexpr int kChunkCta = 2048;     // in-neighbours per CTA work item
+constexpr int kChunkWarp = 256;     // in-neighbours per warp work item
+constexpr int kCtaThreads = 512;    // threads per CTA of the bitmap kernels
+constexpr int kHashSlots = 512;     // slots per warp-private hash table
+constexpr int kHashCap = 256;       // max pivot set size for the hash kernel
+constexpr int kWarpCtaWarps = 8;    // warps per CTA of the warp kernels
+
+enum WarpMode { kModeHash = 0, kModeMerge = 1, kModeGallop = 2 };
+
+struct Item {
+    int32_t pos;  // plist position of the pivot
+    int32_t j0;   // first in-neighbour (index into N-(b))
+};
+
+__device__ __forceinline__ int32_t pivot_at(const int32_t* __restrict__ plist, int64_t p) {
+    return plist ? plist[p] : (int32_t)p;
+}
+
+// Group-of-G scan of the prefix N(c) & [0, b): the G lanes of a group read G
+// consecutive ids per step (coalesced) and test them against the pivot set.
+// The scan stops at the first id >= b (rows are sorted) and never reads more
+// than lim = dplus[c] ids, so it stays inside row c.
+template <int G, class Test>
+__device__ __forceinline__ uint32_t scan_prefix(const int32_t* __restrict__ row, uint32_t lim, int32_t b, int gl,
+                                                unsigned gmask, Test test) {
+    uint32_t hits = 0;
+    for (uint32_t i = 0; i < lim; i += G) {
+        const uint32_t k = i + gl;
+        const int32_t a = k < lim ? __ldg(row + k) : 0x7fffffff;
+        if (a < b) hits += test(a);
+        int32_t last;
+        if constexpr (G == 1) last = a;
+        else last = __shfl_sync(gmask, a, G - 1, G);
+        if (last >= b) break;
+    }
+    return hits;
+}
+
+// CTA-wide bitmap kernel (persistent grid; one item at a time per CTA).
+template <int G>
+__global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __restrict__ off,
+                                                           const int32_t* __restrict__ adj,
+                                                           const uint32_t* __restrict__ dplus,
+                                                           const int32_t* __restrict__ plist,
+                                                           const Item* __restrict__ items,
+                                                           const uint32_t* __restrict__ nitems_p,
+                                                           uint32_t* __restrict__ next_item,
+                                                           unsigned long long* __restrict__ total,
+                                                           uint32_t bm_words) {
+    extern __shared__ uint32_t bm[];
+    __shared__ uint32_t s_item;
+    __shared__ unsigned long long s_sum;
+    const int tid = threadIdx.x;
+    for (uint32_t i = tid; i < bm_words; i += blockDim.x) bm[i] = 0;
+    if (tid == 0) s_sum = 0;
+    const uint32_t nitems = *nitems_p;
+    const int lane = tid & 31;
+    const int group = tid / G, ngroups = blockDim.x / G, gl = tid % G;
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
+    unsigned long long cnt = 0;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(next_item, 1u);
+        __syncthreads();
+        const uint32_t it = s_item;
+        if (it >= nitems) break;
+        const Item I = items[it];
+        const int32_t b = pivot_at(plist, I.pos);
+        const uint64_t rb = off[b], re = off[b + 1];
+        const uint32_t dp = dplus[b];
+        for (uint32_t k = tid; k < dp; k += blockDim.x) {
+            const int32_t a = adj[rb + k];
+            atomicOr(&bm[a >> 5], 1u << (a & 31));
+        }
+        __syncthreads();
+        const uint64_t in0 = rb + dp + (uint64_t)I.j0;
+        const uint64_t in1 = min(in0 + (uint64_t)kChunkCta, re);
+        for (uint64_t e = in0 + group; e < in1; e += ngroups) {
+            const int32_t c = adj[e];
+            cnt += scan_prefix<G>(adj + off[c], dplus[c], b, gl, gmask,
+                                  [&](int32_t a) -> uint32_t { return (bm[a >> 5] >> (a & 31)) & 1u; });
+        }
+        __syncthreads();
+        for (uint32_t k = tid; k < dp; k += blockDim.x) bm[adj[rb + k] >> 5] = 0;
+    }
+    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0 && cnt) atomicAdd(&s_sum, cnt);
+    __syncthreads();
+    if (tid == 0 && s_sum) atomicAdd(total, s_sum);
+}
+
+__device__ __forceinline__ uint32_t hash_slot(int32_t a) { return ((uint32_t)a * 0x9E3779B1u) >> (32 - 9); }
+
+// |x & y & [0, thr)| for sorted x, y: Partitioned_Graph::
+// cnt_common_neis_less_than_merge (src/Graph.cpp:1132-1153), without its
+// one-past-the-end reads.
+__device__ __forceinline__ uint32_t merge_below(const int32_t* __restrict__ x, uint32_t nx,
+                                                const int32_t* __restrict__ y, uint32_t ny, int32_t thr) {
+    uint32_t i = 0, j = 0, c = 0;
+    while (i < nx && j < ny) {
+        const int32_t a = x[i], bb = y[j];
+        if (a >= thr || bb >= thr) break;
+        if (a < bb) ++i;
+        else if (a > bb) ++j;
+        else { ++c; ++i; ++j; }
+    }
+    return c;
+}
+
+// Each id of N(c) & [0, thr) looked up in N+(b) by binary search: the
+// lower_bound probing of Partitioned_Graph::cnt_common_neis_galloping
+// (src/Graph.cpp:1071-1085).
+__device__ __forceinline__ uint32_t gallop_below(const int32_t* __restrict__ x, uint32_t nx,
+                                                 const int32_t* __restrict__ y, uint32_t ny, int32_t thr) {
+    uint32_t c = 0;
+    for (uint32_t i = 0; i < nx; ++i) {
+        const int32_t a = x[i];
+        if (a >= thr) break;
+        uint32_t lo = 0, hi = ny;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (y[mid] < a) lo = mid + 1; else hi = mid;
+        }
+        c += (lo < ny && y[lo] == a) ? 1u : 0u;
+    }
+    return c;
+}
+
+// Warp kernels: one item (pivot, <= kChunkWarp in-neighbours) per warp, one
+// lane per in-neighbour.
+template <int MODE>
+__global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* __restrict__ off,
+                                                                const int32_t* __restrict__ adj,
+                                                                const uint32_t* __restrict__ dplus,
+                                                                const int32_t* __restrict__ plist,
+                                                                const Item* __restrict__ items,
+                                                                const uint32_t* __restrict__ nitems_p,
+                                                                uint32_t* __restrict__ next_item,
+                                                                unsigned long long* __restrict__ total) {
+    __shared__ int32_t table[MODE == kModeHash ? kWarpCtaWarps : 1][MODE == kModeHash ? kHashSlots : 1];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int32_t* T = table[MODE == kModeHash ? w : 0];
+    if (MODE == kModeHash) {
+        for (int s = lane; s < kHashSlots; s += 32) T[s] = -1;
+        __syncwarp();
+    }
+    const uint32_t nitems = *nitems_p;
+    unsigned long long cnt = 0;
+    for (;;) {
+        uint32_t it = 0;
+        if (lane == 0) it = atomicAdd(next_item, 1u);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= nitems) break;
+        const Item I = items[it];
+        const int32_t b = pivot_at(plist, I.pos);
+        const uint64_t rb = off[b], re = off[b + 1];
+        const uint32_t dp = dplus[b];
+        const uint64_t in0 = rb + dp + (uint64_t)I.j0;
+        const uint64_t in1 = min(in0 + (uint64_t)kChunkWarp, re);
+        const int32_t* nb = adj + rb;
+        if (MODE == kModeHash && dp <= (uint32_t)kHashCap) {
+            for (uint32_t k = lane; k < dp; k += 32) {
+                const int32_t a = nb[k];
+                uint32_t s = hash_slot(a);
+                while (atomicCAS(&T[s], -1, a) != -1) s = (s + 1) & (kHashSlots - 1);
+            }
+            __syncwarp();
+            for (uint64_t e = in0 + lane; e < in1; e += 32) {
+                const int32_t c = adj[e];
+                const int32_t* row = adj + off[c];
+                const uint32_t lim = dplus[c];
+                for (uint32_t i = 0; i < lim; ++i) {
+                    const int32_t a = __ldg(row + i);
+                    if (a >= b) break;
+                    uint32_t s = hash_slot(a);
+                    int32_t key;
+                    while ((key = T[s]) != -1) {
+                        if (key == a) { ++cnt; break; }
+                        s = (s + 1) & (kHashSlots - 1);
+                    }
+                }
+            }
+            __syncwarp();
+            for (int s = lane; s < kHashSlots; s += 32) T[s] = -1;
+            __syncwarp();
+        } else if (MODE == kModeGallop) {
+            for (uint64_t e = in0 + lane; e < in1; e += 32) {
+                const int32_t c = adj[e];
+                cnt += gallop_below(adj + off[c], dplus[c], nb, dp, b);
+            }
+        } else {
+            for (uint64_t e = in0 + lane; e < in1; e += 32) {
+                const int32_t c = adj[e];
+                cnt += merge_below(adj + off[c], dplus[c], nb, dp, b);
+            }
+        }
+    }
+    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0 && cnt) atomicAdd(total, cnt);
+}
+
+}  // namespace tc
+}  // namespace pc
