@@ -70,8 +70,9 @@ pc_status pc_host_unregister(void* ptr);
  * (src/Graph.cpp:92-137) and Graph::Graph(adj_list) (src/Graph.cpp:139-149):
  * the arrays are exactly the contents of csr_vlist.bin / csr_elist.bin /
  * csr_weight.bin.  Unless PC_GRAPH_NO_VALIDATE, the device checks that
- * offsets are monotone, ids in range, rows strictly ascending, no self-loops
- * and the adjacency symmetric, and returns PC_ERR_INVALID_INPUT otherwise. */
+ * offsets are monotone, ids in range, rows strictly ascending, no self-loops,
+ * the adjacency symmetric (a two-way 64-bit fingerprint of the edge multiset)
+ * and weights in [0, 2^30), and returns PC_ERR_INVALID_INPUT otherwise. */
 pc_status pc_graph_create(const uint64_t* vlist, const int32_t* elist, const int32_t* weights,
                           uint64_t n, uint64_t m, uint32_t flags, pc_graph** out);
 pc_status pc_graph_destroy(pc_graph* g);
@@ -260,6 +261,8 @@ pc_status pc_host_csr_save(const pc_host_csr* g, const char* dir);
 pc_status pc_host_csr_from_arrays(const uint64_t* vlist, const int32_t* elist, const int32_t* weights,
                                   uint64_t n, uint64_t m, pc_host_csr** out);
 pc_status pc_host_csr_free(pc_host_csr* g);
+/* The priorities pc_mis_hashed orders vertices by: out[v] for v < n. */
+pc_status pc_synth_vertex_priority(uint64_t seed, uint64_t n, uint64_t* out);
 
 #ifdef __cplusplus
 }

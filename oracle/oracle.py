@@ -37,6 +37,26 @@ def _ptr(a):
     return None if a is None else C.c_void_p(a.ctypes.data)
 
 
+class _Mute:
+    """Sends the process's stdout (fd 1) to /dev/null while the reference's
+    own printf progress lines run, so callers keep a clean stdout."""
+
+    def __enter__(self):
+        import sys
+        sys.stdout.flush()
+        C.CDLL(None).fflush(None)
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *a):
+        C.CDLL(None).fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
 def _load_c():
     if not ORACLE_SO.exists():
         build(ref=False)
@@ -44,6 +64,7 @@ def _load_c():
     sig = {
         "or_tc_merge": (u64, [u64, P, P]),
         "or_tc_galloping": (u64, [u64, P, P]),
+        "or_tc_rows": (u64, [u64, P, P, P, u64]),
         "or_layout": (C.c_int, [u64, P, P, P, P, i32, P, P, P]),
         "or_tc_partitioned": (u64, [u64, P, P, i32]),
         "or_lcc": (None, [u64, P, P, P]),
@@ -87,6 +108,12 @@ def _csr(vl, el):
 def tc_merge(vl, el):
     vl, el, n = _csr(vl, el)
     return int(clib().or_tc_merge(n, _ptr(vl), _ptr(el)))
+
+
+def tc_rows(vl, el, rows):
+    vl, el, n = _csr(vl, el)
+    r = np.ascontiguousarray(rows, np.int32)
+    return int(clib().or_tc_rows(n, _ptr(vl), _ptr(el), _ptr(r), r.size))
 
 
 def tc_galloping(vl, el):
@@ -202,6 +229,15 @@ def cdlp(vl, el, labels, iters=10):
 
 # ---- the reference itself (oracle/_ref) ------------------------------------------
 
+def _muted(fn):
+    def wrap(*a, **k):
+        with _Mute():
+            return fn(*a, **k)
+    wrap.__name__ = fn.__name__
+    wrap.__doc__ = fn.__doc__
+    return wrap
+
+
 class Reference:
     """The reference library (libpcref.so) on one graph, written to a temporary
     CSR directory in the reference's binary format and loaded by its own
@@ -264,13 +300,15 @@ class Reference:
             np.ascontiguousarray(el, np.int32).tofile(os.path.join(csrdir, "csr_elist.bin"))
             if w is not None:
                 np.ascontiguousarray(w, np.int32).tofile(os.path.join(csrdir, "csr_weight.bin"))
-        self.g = lib.ref_graph_load(csrdir.encode(), int(w is not None))
+        with _Mute():
+            self.g = lib.ref_graph_load(csrdir.encode(), int(w is not None))
         self.n = int(lib.ref_graph_n(self.g))
         self.m = int(lib.ref_graph_m(self.g))
         self.pg = None
         if v2p is not None:
             self.v2p = np.ascontiguousarray(v2p, np.int32)
-            self.pg = lib.ref_pgraph_new(self.g, _ptr(self.v2p), self.n, self.threads)
+            with _Mute():
+                self.pg = lib.ref_pgraph_new(self.g, _ptr(self.v2p), self.n, self.threads)
 
     def close(self):
         lib = self.lib()
@@ -295,16 +333,19 @@ class Reference:
             raise ValueError("no partition given")
         return self.pg if partitioned else self.g
 
+    @_muted
     def tc(self, partitioned=False, galloping=False):
         lib = self.lib()
         if partitioned:
             return int(lib.ref_tc_pgraph(self.pg, int(galloping)))
         return int(lib.ref_tc_graph(self.g, int(galloping), self.threads))
 
+    @_muted
     def tc_rows(self, rows):
         r = np.ascontiguousarray(rows, np.int32)
         return int(self.lib().ref_tc_rows(self.g, _ptr(r), r.size, self.threads))
 
+    @_muted
     def layout(self):
         P_ = int(self.lib().ref_pgraph_partitions(self.pg))
         vl = np.empty(P_ * self.n + 1, np.uint64)
@@ -312,9 +353,11 @@ class Reference:
         self.lib().ref_pgraph_layout(self.pg, _ptr(vl), _ptr(el), None)
         return vl, el
 
+    @_muted
     def reorder(self):
         self.lib().ref_pgraph_reorder(self.pg)
 
+    @_muted
     def lcc(self, partitioned=False, galloping=False):
         out = np.empty(self.n, np.float64)
         if partitioned:
@@ -323,6 +366,7 @@ class Reference:
             self.lib().ref_lcc_graph(self.g, int(galloping), self.threads, _ptr(out))
         return out
 
+    @_muted
     def jsim(self, q, partitioned=False):
         q = np.ascontiguousarray(q, np.int32)
         out = np.empty(q.size * q.size, np.float64)
@@ -332,6 +376,7 @@ class Reference:
             self.lib().ref_jsim_graph(self.g, _ptr(q), q.size, self.threads, _ptr(out))
         return out
 
+    @_muted
     def batch_pairs(self, pairs, partitioned=False):
         p = np.ascontiguousarray(pairs, np.int32).reshape(-1)
         out = np.empty(p.size // 2, np.uint64)
@@ -339,6 +384,7 @@ class Reference:
                                    _ptr(out))
         return out
 
+    @_muted
     def batch_sets(self, sets, partitioned=False):
         ids = np.concatenate([np.asarray(s, np.int32) for s in sets])
         offs = np.zeros(len(sets) + 1, np.uint64)
@@ -348,32 +394,38 @@ class Reference:
                                   self.threads, _ptr(out))
         return out
 
+    @_muted
     def bfs_parents(self, src):
         out = np.empty(self.n, np.int32)
         self.lib().ref_bfs_graph(self.g, src, _ptr(out))
         return out
 
+    @_muted
     def sssp(self, src, partitioned=False):
         out = np.empty(self.n, np.int32)
         self.lib().ref_sssp(self._obj(partitioned), int(partitioned), self.n, src, _ptr(out))
         return out
 
+    @_muted
     def pagerank(self, damping=0.85, iters=20, partitioned=True):
         out = np.empty(self.n, np.float32)
         self.lib().ref_pagerank(self._obj(partitioned), int(partitioned), self.n, damping, iters, self.threads,
                                 _ptr(out))
         return out
 
+    @_muted
     def kcore(self, partitioned=False):
         out = np.empty(self.n, np.int32)
         self.lib().ref_kcore(self._obj(partitioned), int(partitioned), self.n, self.threads, _ptr(out))
         return out
 
+    @_muted
     def mis(self, partitioned=False):
         out = np.empty(self.n, np.int32)
         self.lib().ref_mis(self._obj(partitioned), int(partitioned), self.n, self.threads, _ptr(out))
         return out
 
+    @_muted
     def cdlp(self, labels, iters=10, partitioned=False):
         lab = np.ascontiguousarray(labels, np.int32).copy()
         self.lib().ref_cdlp(self._obj(partitioned), int(partitioned), self.n, iters, self.threads, _ptr(lab))

@@ -52,6 +52,23 @@ uint64_t or_tc_merge(uint64_t n, const uint64_t* vl, const int32_t* el) {
     return res;
 }
 
+/* The loop of Graph::solve_triangle_counting_merge (src/Graph.cpp:358-365)
+ * restricted to the given rows (a bounded sample for timing). */
+uint64_t or_tc_rows(uint64_t n, const uint64_t* vl, const int32_t* el, const int32_t* rows, uint64_t nrows) {
+    (void)n;
+    uint64_t res = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : res)
+    for (int64_t i = 0; i < (int64_t)nrows; i++) {
+        int64_t u = rows[i];
+        for (uint64_t j = vl[u]; j < vl[u + 1]; j++) {
+            int32_t v = el[j];
+            if (u <= v) continue;
+            res += lt_merge(vl, el, u, v, v);
+        }
+    }
+    return res;
+}
+
 /* Graph::solve_triangle_counting_galloping (src/Graph.cpp:342-353) with
  * Graph::cnt_common_neis_galloping (src/Graph.cpp:186-198): every ordered
  * edge, each element of the shorter list binary-searched in the longer. */
@@ -315,7 +332,8 @@ void or_pagerank_f64(uint64_t n, const uint64_t* vl, const int32_t* el, double d
 }
 
 /* Core numbers as Graph::solve_kcore peels them (src/Graph.cpp:662-719): a
- * vertex removed while peeling level k (degree < k) has core number k - 1.
+ * vertex removed while peeling level k (degree < k) has core number k - 1,
+ * for levels k < n.
  * Computed with the O(m) bucket order of Batagelj & Zaversnik (2003), which
  * yields the same numbers. */
 int32_t or_kcore(uint64_t n, const uint64_t* vl, const int32_t* el, int32_t* core) {
@@ -353,6 +371,16 @@ int32_t or_kcore(uint64_t n, const uint64_t* vl, const int32_t* el, int32_t* cor
         }
     }
     free(deg); free(bin); free(pos); free(vert);
+    /* The reference peels levels k = 1 .. n-1 only (src/Graph.cpp:683): a
+     * vertex still present after level n-1 keeps its initial 0.  That happens
+     * exactly when the graph is complete (core number n-1 everywhere). */
+    if (n >= 2 && largest >= (int32_t)n - 1) {
+        largest = 0;
+        for (uint64_t u = 0; u < n; u++) {
+            if (core[u] >= (int32_t)n - 1) core[u] = 0;
+            if (core[u] > largest) largest = core[u];
+        }
+    }
     return largest;
 }
 

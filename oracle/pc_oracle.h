@@ -9,6 +9,7 @@ extern "C" {
 
 uint64_t or_tc_merge(uint64_t n, const uint64_t* vl, const int32_t* el);
 uint64_t or_tc_galloping(uint64_t n, const uint64_t* vl, const int32_t* el);
+uint64_t or_tc_rows(uint64_t n, const uint64_t* vl, const int32_t* el, const int32_t* rows, uint64_t nrows);
 int or_layout(uint64_t n, const uint64_t* vl, const int32_t* el, const int32_t* w, const int32_t* v2p, int32_t P,
               uint64_t* out_vl, int32_t* out_el, int32_t* out_w);
 uint64_t or_tc_partitioned(uint64_t n, const uint64_t* pvl, const int32_t* pel, int32_t P);

@@ -36,6 +36,13 @@ def launch_count() -> int:
     return int(lib.pc_launch_count())
 
 
+def vertex_priority(seed: int, n: int) -> np.ndarray:
+    """Priorities Partitioned_Graph.solve_mis(seed=...) orders vertices by."""
+    out = np.empty(n, np.uint64)
+    check(lib.pc_synth_vertex_priority(seed, n, ptr(out)))
+    return out
+
+
 def equal_vertex_partition(n: int, P: int) -> np.ndarray:
     """part(u) = floor(u * P / n): P contiguous blocks of equal vertex count."""
     return ((np.arange(n, dtype=np.int64) * P) // max(n, 1)).astype(np.int32)

@@ -129,6 +129,7 @@ _SIG = {
     "pc_host_csr_save": (i32, [P, C.c_char_p]),
     "pc_host_csr_from_arrays": (i32, [P, P, P, u64, u64, PP]),
     "pc_host_csr_free": (i32, [P]),
+    "pc_synth_vertex_priority": (i32, [u64, u64, P]),
 }
 
 

@@ -19,6 +19,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libpc.so"
+BIN = PKG / "bin"
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -84,6 +85,13 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
         tmp = LIB.with_suffix(".so.tmp")
         _run([NVCC] + ARCH + ["-shared", "-o", str(tmp)] + [str(o) for o in objs] + ["-Xcompiler", "-fopenmp", "-lgomp"])
         os.replace(tmp, LIB)
+    # command-line tools linked against the library (rpath to the package dir)
+    BIN.mkdir(exist_ok=True)
+    for src in sorted((CSRC / "tools").glob("*.cpp")):
+        exe = BIN / src.stem
+        if force or jobs or not exe.exists() or src.stat().st_mtime > exe.stat().st_mtime:
+            _run([CXX, "-O3", "-std=c++17", "-Wall", "-I", str(ROOT / "include"), str(src), "-o", str(exe),
+                  "-L", str(PKG), "-lpc", "-Wl,-rpath,$ORIGIN/.."])
     if verbose:
         for o in outputs:
             if o.strip():

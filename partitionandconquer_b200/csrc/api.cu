@@ -100,6 +100,7 @@ enum : uint32_t {
     BAD_RANGE = 2u,
     BAD_ORDER = 4u,
     BAD_SELF = 8u,
+    BAD_WEIGHT = 16u,
 };
 
 __global__ void k_check_offsets(const uint64_t* __restrict__ off, uint64_t n, uint64_t m, uint32_t* err) {
@@ -176,6 +177,16 @@ __global__ void k_check_edges(const uint64_t* __restrict__ off, const int32_t* _
         if (acc1) atomicAdd(&fp[1], (unsigned long long)acc1);
         if (bad) atomicOr(err, bad);
     }
+}
+
+// Weights must be in [0, 2^30): non-negative for the shortest-path semantics,
+// and small enough that a distance plus a weight cannot overflow int32.
+__global__ void k_check_weights(const int32_t* __restrict__ w, uint64_t m, uint32_t* err) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    bool bad = false;
+    for (; i < m; i += stride) bad |= (w[i] < 0 || w[i] >= (1 << 30));
+    if (bad) atomicOr(err, BAD_WEIGHT);
 }
 
 // ---- kernels: partition layout export ---------------------------------------
@@ -255,6 +266,29 @@ static pc_status gather_to_api(pc_pgraph* pg, const T* in, T* out) {
 pc_status gather_to_api_i32(pc_pgraph* pg, const int32_t* in, int32_t* out) { return gather_to_api(pg, in, out); }
 pc_status gather_to_api_f32(pc_pgraph* pg, const float* in, float* out) { return gather_to_api(pg, in, out); }
 pc_status gather_to_api_f64(pc_pgraph* pg, const double* in, double* out) { return gather_to_api(pg, in, out); }
+
+template <class T>
+static pc_status gather_to_internal(pc_pgraph* pg, const T* in, T* out) {
+    uint64_t n = pg->g->n;
+    if (api_is_internal(pg)) {
+        if (in != out) PC_CUDA(cudaMemcpyAsync(out, in, n * sizeof(T), cudaMemcpyDeviceToDevice, pg->g->stream));
+        return PC_OK;
+    }
+    // out[internal u] = in[API id of u] = in[old2new[u]]
+    k_gather<T><<<(unsigned)ceil_div(n, 256), 256, 0, pg->g->stream>>>(in, pg->old2new.as<int32_t>(), n, out);
+    PC_LAUNCHED();
+    return PC_OK;
+}
+pc_status gather_to_internal_i32(pc_pgraph* pg, const int32_t* in, int32_t* out) { return gather_to_internal(pg, in, out); }
+pc_status gather_to_internal_f32(pc_pgraph* pg, const float* in, float* out) { return gather_to_internal(pg, in, out); }
+pc_status gather_to_internal_f64(pc_pgraph* pg, const double* in, double* out) { return gather_to_internal(pg, in, out); }
+
+int32_t to_internal_id(const pc_pgraph* pg, int32_t api_id) {
+    if (api_is_internal(pg)) return api_id;
+    int32_t v = 0;
+    cudaMemcpy(&v, pg->new2old.as<int32_t>() + api_id, 4, cudaMemcpyDeviceToHost);
+    return v;
+}
 
 pc_status ensure_dplus(pc_pgraph* pg) {
     if (pg->dplus.p) return PC_OK;
@@ -366,6 +400,10 @@ pc_status pc_graph_create(const uint64_t* vlist, const int32_t* elist, const int
         if (m) {
             k_check_edges<<<sms * 8, 256, 0, g->stream>>>(g->off.as<uint64_t>(), g->adj.as<int32_t>(), n, m, d_err, d_fp);
             count_launch();
+            if (g->weighted) {
+                k_check_weights<<<sms * 4, 256, 0, g->stream>>>(g->w.as<int32_t>(), m, d_err);
+                count_launch();
+            }
         }
         uint64_t h_fp[2] = {0, 0};
         e = cudaMemcpyAsync(&h_err, d_err, 4, cudaMemcpyDeviceToHost, g->stream);
@@ -377,6 +415,7 @@ pc_status pc_graph_create(const uint64_t* vlist, const int32_t* elist, const int
         if (h_err & BAD_ORDER)
             return cleanup(fail(PC_ERR_INVALID_INPUT, "neighbour lists must be strictly ascending (sorted, no duplicates)"));
         if (h_fp[0] || h_fp[1]) return cleanup(fail(PC_ERR_INVALID_INPUT, "the adjacency is not symmetric"));
+        if (h_err & BAD_WEIGHT) return cleanup(fail(PC_ERR_INVALID_INPUT, "edge weights must be in [0, 2^30)"));
     } else {
         e = cudaStreamSynchronize(g->stream);
         if (e != cudaSuccess) return cleanup(cuda_fail(e, "upload", __FILE__, __LINE__));

@@ -1,0 +1,647 @@
+// Frontier algorithms: BFS, SSSP, PageRank, k-core, MIS, CDLP (sm_100a).
+//
+// All kernels work on the symmetric CSR in the internal id space; inputs and
+// outputs are mapped to the caller's id space (identity unless the view was
+// reordered).  Frontiers are compacted queues; appends are warp-aggregated
+// (one atomic per warp and step).
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <vector>
+
+#include "pc_internal.cuh"
+#include "synth_rng.h"
+
+namespace pc {
+namespace fr {
+
+constexpr int kThreads = 256;
+constexpr int32_t kInf = INT_MAX;
+
+// Appends `val` for every lane with pred set; all 32 lanes of the warp must
+// call it together.
+__device__ __forceinline__ void warp_append(bool pred, int32_t val, int32_t* __restrict__ q,
+                                            uint32_t* __restrict__ qn) {
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(qn, (uint32_t)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (pred) q[base + __popc(m & ((1u << lane) - 1u))] = val;
+}
+
+__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t x) {
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+// ---- BFS -------------------------------------------------------------------
+
+__global__ void k_iota(int32_t* a, uint64_t n) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < n) a[i] = (int32_t)i;
+}
+
+__global__ void k_fill_i32(int32_t* a, uint64_t n, int32_t v) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
+
+// Top-down step: one warp per frontier vertex, lanes over its neighbours.
+__global__ void k_bfs_top_down(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                               const int32_t* __restrict__ fq, uint32_t fn, int32_t* __restrict__ dist,
+                               int32_t level, int32_t* __restrict__ nq, uint32_t* __restrict__ nn,
+                               unsigned long long* __restrict__ next_edges) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    uint64_t edges = 0;
+    for (uint64_t i = warp; i < fn; i += nwarps) {
+        const int32_t u = fq[i];
+        const uint64_t b = off[u], e = off[u + 1];
+        for (uint64_t j0 = b; j0 < e; j0 += 32) {
+            const uint64_t j = j0 + lane;
+            bool won = false;
+            int32_t v = 0;
+            if (j < e) {
+                v = adj[j];
+                if (dist[v] == kInf) won = atomicCAS(&dist[v], kInf, level) == kInf;
+            }
+            if (won) edges += off[v + 1] - off[v];
+            warp_append(won, v, nq, nn);
+        }
+    }
+    edges = warp_sum_u64(edges);
+    if (lane == 0 && edges) atomicAdd(next_edges, (unsigned long long)edges);
+}
+
+// Bottom-up step: every unvisited vertex looks for a neighbour at level-1.
+__global__ void k_bfs_bottom_up(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj, uint64_t n,
+                                int32_t* __restrict__ dist, int32_t level, int32_t* __restrict__ nq,
+                                uint32_t* __restrict__ nn, unsigned long long* __restrict__ next_edges) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t nr = (n + 31) & ~31ull;
+    uint64_t edges = 0;
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < nr; v += stride) {
+        bool found = false;
+        if (v < n && dist[v] == kInf) {
+            const uint64_t b = off[v], e = off[v + 1];
+            for (uint64_t j = b; j < e; ++j) {
+                if (dist[adj[j]] == level - 1) { found = true; break; }
+            }
+            if (found) {
+                dist[v] = level;
+                edges += e - b;
+            }
+        }
+        warp_append(found, (int32_t)v, nq, nn);
+    }
+    edges = warp_sum_u64(edges);
+    if ((threadIdx.x & 31) == 0 && edges) atomicAdd(next_edges, (unsigned long long)edges);
+}
+
+__global__ void k_bfs_finish(const int32_t* __restrict__ dist, uint64_t n, int32_t* __restrict__ rank) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < n) rank[i] = dist[i] == 0 ? -1 : dist[i];
+}
+
+// ---- SSSP (frontier Bellman-Ford) --------------------------------------------
+
+__global__ void k_sssp_relax(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                             const int32_t* __restrict__ w, const int32_t* __restrict__ fq, uint32_t fn,
+                             int32_t* __restrict__ dist, int32_t* __restrict__ flag, int32_t* __restrict__ nq,
+                             uint32_t* __restrict__ nn) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = warp; i < fn; i += nwarps) {
+        const int32_t u = fq[i];
+        const int32_t du = dist[u];
+        const uint64_t b = off[u], e = off[u + 1];
+        for (uint64_t j0 = b; j0 < e; j0 += 32) {
+            const uint64_t j = j0 + lane;
+            bool push = false;
+            int32_t v = 0;
+            if (j < e) {
+                v = adj[j];
+                const int32_t nd = du + w[j];
+                if (nd < dist[v]) {
+                    const int32_t old = atomicMin(&dist[v], nd);
+                    if (nd < old) push = atomicExch(&flag[v], 1) == 0;
+                }
+            }
+            warp_append(push, v, nq, nn);
+        }
+    }
+}
+
+__global__ void k_clear_flags(const int32_t* __restrict__ q, uint32_t qn, int32_t* __restrict__ flag) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < qn) flag[q[i]] = 0;
+}
+
+// ---- PageRank (pull) -----------------------------------------------------------
+
+template <class T>
+__global__ void k_pr_init(const uint64_t* __restrict__ off, uint64_t n, T damping, const T* __restrict__ init,
+                          T* __restrict__ degs, T* __restrict__ contrib) {
+    uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (u >= n) return;
+    // degs[u] = d(u) / damping; x0 = degs / n (src/Graph.cpp:1563-1570)
+    const T dg = (T)(off[u + 1] - off[u]) / damping;
+    degs[u] = dg;
+    const T x0 = init ? init[u] : dg / (T)n;
+    contrib[u] = dg > (T)0 ? x0 / dg : (T)0;
+}
+
+// One iteration: x'[v] = base + sum_{u in N(v)} contrib[u]; contrib'[v] = x'[v] / degs[v].
+template <class T>
+__global__ void k_pr_iter(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj, uint64_t n, T base,
+                          const T* __restrict__ degs, const T* __restrict__ contrib, T* __restrict__ x_out,
+                          T* __restrict__ contrib_out) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = warp; v < n; v += nwarps) {
+        const uint64_t b = off[v], e = off[v + 1];
+        T s = (T)0;
+        for (uint64_t j = b + lane; j < e; j += 32) s += __ldg(contrib + adj[j]);
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) {
+            const T x = base + s;
+            x_out[v] = x;
+            const T dg = degs[v];
+            contrib_out[v] = dg > (T)0 ? x / dg : (T)0;
+        }
+    }
+}
+
+// ---- k-core ----------------------------------------------------------------------
+
+__global__ void k_kcore_init(const uint64_t* __restrict__ off, uint64_t n, int32_t* __restrict__ deg,
+                             int32_t* __restrict__ core, int32_t* __restrict__ rem) {
+    uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (u >= n) return;
+    deg[u] = (int32_t)(off[u + 1] - off[u]);
+    core[u] = -1;
+    rem[u] = (int32_t)u;
+}
+
+// Scan of the remaining vertices at level k: degree < k -> core k-1, into the
+// peel queue; others stay (compacted).  Also returns the minimum degree left.
+__global__ void k_kcore_scan(const int32_t* __restrict__ rem, uint32_t rn, int32_t k, int32_t* __restrict__ deg,
+                             int32_t* __restrict__ core, int32_t* __restrict__ fq, uint32_t* __restrict__ fn,
+                             int32_t* __restrict__ rem2, uint32_t* __restrict__ rn2, int32_t* __restrict__ min_left) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t nr = (rn + 31) & ~31u;
+    int32_t mn = INT_MAX;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nr; i += stride) {
+        bool peel = false, keep = false;
+        int32_t u = 0;
+        if (i < rn) {
+            u = rem[i];
+            if (core[u] < 0) {
+                if (deg[u] < k) { peel = true; core[u] = k - 1; }
+                else { keep = true; mn = min(mn, deg[u]); }
+            }
+        }
+        warp_append(peel, u, fq, fn);
+        warp_append(keep, u, rem2, rn2);
+    }
+    for (int o = 16; o; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    if ((threadIdx.x & 31) == 0 && mn != INT_MAX) atomicMin(min_left, mn);
+}
+
+// Peeling step: neighbours of peeled vertices lose one degree; a neighbour
+// whose degree crosses from k to k-1 is peeled next (exactly once).
+__global__ void k_kcore_peel(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                             const int32_t* __restrict__ fq, uint32_t fn, int32_t k, int32_t* __restrict__ deg,
+                             int32_t* __restrict__ core, int32_t* __restrict__ nq, uint32_t* __restrict__ nn) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = warp; i < fn; i += nwarps) {
+        const int32_t u = fq[i];
+        const uint64_t b = off[u], e = off[u + 1];
+        for (uint64_t j0 = b; j0 < e; j0 += 32) {
+            const uint64_t j = j0 + lane;
+            bool push = false;
+            int32_t v = 0;
+            if (j < e) {
+                v = adj[j];
+                if (core[v] < 0) {
+                    const int32_t old = atomicSub(&deg[v], 1);
+                    if (old == k) { push = true; core[v] = k - 1; }
+                }
+            }
+            warp_append(push, v, nq, nn);
+        }
+    }
+}
+
+__global__ void k_kcore_unpeeled(int32_t* __restrict__ core, uint64_t n) {
+    uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (u < n && core[u] < 0) core[u] = 0;
+}
+
+// ---- MIS -------------------------------------------------------------------------
+
+// Round over the undecided list: OUT if a neighbour is IN; IN if every
+// neighbour of smaller priority is OUT; otherwise undecided again.  Decisions
+// are final and only made from final neighbour states, so the in-place update
+// reaches the unique greedy (lexicographically-first) set.
+__global__ void k_mis_round(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                            const uint64_t* __restrict__ prio, const int32_t* __restrict__ uq, uint32_t un,
+                            int32_t* __restrict__ state, int32_t* __restrict__ nq, uint32_t* __restrict__ nn) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = warp; i < un; i += nwarps) {
+        const int32_t u = uq[i];
+        const uint64_t pu = prio ? prio[u] : (uint64_t)u;
+        const uint64_t b = off[u], e = off[u + 1];
+        bool in_nbr = false, blocked = false;
+        for (uint64_t j0 = b; j0 < e; j0 += 32) {
+            const uint64_t j = j0 + lane;
+            bool a = false, c = false;
+            if (j < e) {
+                const int32_t v = adj[j];
+                const int32_t sv = state[v];
+                a = sv == 1;
+                const uint64_t pv = prio ? prio[v] : (uint64_t)v;
+                c = sv == 0 && (pv < pu || (pv == pu && v < u));
+            }
+            in_nbr = __any_sync(0xffffffffu, a) || in_nbr;
+            blocked = __any_sync(0xffffffffu, c) || blocked;
+            if (in_nbr) break;
+        }
+        if (lane == 0) {
+            if (in_nbr) state[u] = 2;
+            else if (!blocked) state[u] = 1;
+        }
+        const bool again = !in_nbr && blocked;
+        if (lane == 0 && again) nq[atomicAdd(nn, 1u)] = u;
+    }
+}
+
+__global__ void k_mis_prio(uint64_t n, const int32_t* __restrict__ int2api, uint64_t key, int hashed,
+                           uint64_t* __restrict__ prio) {
+    uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (u >= n) return;
+    const uint32_t api = int2api ? (uint32_t)int2api[u] : (uint32_t)u;
+    prio[u] = hashed ? pc_vertex_priority(key, api) : (uint64_t)api;
+}
+
+__global__ void k_mis_finish(const int32_t* __restrict__ state, uint64_t n, int32_t* __restrict__ res) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < n) res[i] = state[i] == 1 ? 1 : 0;
+}
+
+// ---- CDLP --------------------------------------------------------------------------
+
+__global__ void k_cdlp_iter(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj, uint64_t n,
+                            const int32_t* __restrict__ lab, int32_t* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = warp; v < n; v += nwarps) {
+        const uint64_t b = off[v], e = off[v + 1];
+        int32_t mx = 0;  // src/Graph.cpp:650: labels start at 0 for every vertex
+        for (uint64_t j = b + lane; j < e; j += 32) mx = max(mx, __ldg(lab + adj[j]));
+        for (int o = 16; o; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0) out[v] = mx;
+    }
+}
+
+}  // namespace fr
+
+using namespace fr;
+
+static unsigned grid_for(const pc_pgraph* pg, int per_sm = 8) { return (unsigned)(sm_count(pg->g->device) * per_sm); }
+
+// Reads a device counter (synchronising the stream).
+static pc_status read_u32(pc_pgraph* pg, const uint32_t* d, uint32_t* h) {
+    PC_CUDA(cudaMemcpyAsync(h, d, 4, cudaMemcpyDeviceToHost, pg->g->stream));
+    PC_CUDA(cudaStreamSynchronize(pg->g->stream));
+    return PC_OK;
+}
+
+static pc_status bfs_run(pc_pgraph* pg, int32_t src, int32_t* rank_host) {
+    const uint64_t n = pg->g->n, m = pg->g->m;
+    cudaStream_t s = pg->g->stream;
+    PC_TRY(scratch_reserve(pg, n * 4 * 4 + 256));
+    int32_t* dist = pg->scratch.take<int32_t>(n);
+    int32_t* q0 = pg->scratch.take<int32_t>(n);
+    int32_t* q1 = pg->scratch.take<int32_t>(n);
+    uint32_t* cnt = pg->scratch.take<uint32_t>(4);
+    unsigned long long* edges = pg->scratch.take<unsigned long long>(2);
+    const unsigned nb = (unsigned)ceil_div(n, kThreads);
+    k_fill_i32<<<nb, kThreads, 0, s>>>(dist, n, kInf);
+    PC_LAUNCHED();
+    const int32_t zero = 0;
+    PC_CUDA(cudaMemcpyAsync(dist + src, &zero, 4, cudaMemcpyHostToDevice, s));
+    PC_CUDA(cudaMemcpyAsync(q0, &src, 4, cudaMemcpyHostToDevice, s));
+    // host-side state of the direction heuristic (Beamer, Asanovic, Patterson, SC'12)
+    std::vector<uint64_t> h_off(2);
+    PC_CUDA(cudaMemcpyAsync(h_off.data(), pg->off + src, 16, cudaMemcpyDeviceToHost, s));
+    PC_CUDA(cudaStreamSynchronize(s));
+    uint64_t frontier_edges = h_off[1] - h_off[0];
+    uint64_t unexplored = m - frontier_edges;
+    uint32_t fn = 1;
+    bool bottom_up = false;
+    const double alpha = 15.0, beta = 18.0;
+    int32_t* fq = q0;
+    int32_t* nq = q1;
+    for (int32_t level = 1; fn > 0; ++level) {
+        if (!bottom_up && (double)frontier_edges > (double)unexplored / alpha) bottom_up = true;
+        else if (bottom_up && (double)fn < (double)n / beta) bottom_up = false;
+        PC_CUDA(cudaMemsetAsync(cnt, 0, 4, s));
+        PC_CUDA(cudaMemsetAsync(edges, 0, 8, s));
+        if (bottom_up) {
+            k_bfs_bottom_up<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, n, dist, level, nq, cnt, edges);
+        } else {
+            k_bfs_top_down<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, fq, fn, dist, level, nq, cnt, edges);
+        }
+        PC_LAUNCHED();
+        unsigned long long h_edges = 0;
+        PC_CUDA(cudaMemcpyAsync(&fn, cnt, 4, cudaMemcpyDeviceToHost, s));
+        PC_CUDA(cudaMemcpyAsync(&h_edges, edges, 8, cudaMemcpyDeviceToHost, s));
+        PC_CUDA(cudaStreamSynchronize(s));
+        frontier_edges = h_edges;
+        unexplored = unexplored > h_edges ? unexplored - h_edges : 0;
+        std::swap(fq, nq);
+        if (level > (int32_t)n + 1) return fail(PC_ERR_TIMEOUT, "BFS did not converge");
+    }
+    int32_t* rank_int = q0 == fq ? q1 : q0;  // any free n-array
+    k_bfs_finish<<<nb, kThreads, 0, s>>>(dist, n, rank_int);
+    PC_LAUNCHED();
+    int32_t* rank_api = dist;
+    PC_TRY(gather_to_api_i32(pg, rank_int, rank_api));
+    PC_CUDA(cudaMemcpyAsync(rank_host, rank_api, n * 4, cudaMemcpyDeviceToHost, s));
+    return sync(pg);
+}
+
+template <class T>
+static pc_status pagerank_run(pc_pgraph* pg, T damping, int32_t iters, const T* init, T* out_host) {
+    const uint64_t n = pg->g->n;
+    cudaStream_t s = pg->g->stream;
+    PC_TRY(scratch_reserve(pg, n * sizeof(T) * 6 + 256));
+    T* degs = pg->scratch.take<T>(n);
+    T* c0 = pg->scratch.take<T>(n);
+    T* c1 = pg->scratch.take<T>(n);
+    T* x = pg->scratch.take<T>(n);
+    T* xapi = pg->scratch.take<T>(n);
+    T* ini = nullptr;
+    const unsigned nb = (unsigned)ceil_div(n, kThreads);
+    if (init) {
+        ini = pg->scratch.take<T>(n);
+        PC_CUDA(cudaMemcpyAsync(xapi, init, n * sizeof(T), cudaMemcpyHostToDevice, s));
+        if (sizeof(T) == 4) PC_TRY(gather_to_internal_f32(pg, (const float*)xapi, (float*)ini));
+        else PC_TRY(gather_to_internal_f64(pg, (const double*)xapi, (double*)ini));
+    }
+    k_pr_init<T><<<nb, kThreads, 0, s>>>(pg->off, n, damping, ini, degs, c0);
+    PC_LAUNCHED();
+    // (1 - damping) / n in the working precision (src/Graph.cpp:1558)
+    const T base = ((T)1 - damping) / (T)n;
+    for (int32_t it = 0; it < iters; ++it) {
+        k_pr_iter<T><<<grid_for(pg, 16), kThreads, 0, s>>>(pg->off, pg->adj, n, base, degs, c0, x, c1);
+        PC_LAUNCHED();
+        std::swap(c0, c1);
+    }
+    if (sizeof(T) == 4) PC_TRY(gather_to_api_f32(pg, (const float*)x, (float*)xapi));
+    else PC_TRY(gather_to_api_f64(pg, (const double*)x, (double*)xapi));
+    PC_CUDA(cudaMemcpyAsync(out_host, xapi, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+    return sync(pg);
+}
+
+static pc_status mis_run(pc_pgraph* pg, bool hashed, uint64_t seed, int32_t* res_host) {
+    const uint64_t n = pg->g->n;
+    cudaStream_t s = pg->g->stream;
+    PC_TRY(scratch_reserve(pg, n * 4 * 4 + n * 8 + 256));
+    int32_t* state = pg->scratch.take<int32_t>(n);
+    int32_t* q0 = pg->scratch.take<int32_t>(n);
+    int32_t* q1 = pg->scratch.take<int32_t>(n);
+    int32_t* out = pg->scratch.take<int32_t>(n);
+    uint64_t* prio = nullptr;
+    uint32_t* cnt = pg->scratch.take<uint32_t>(2);
+    const unsigned nb = (unsigned)ceil_div(n, kThreads);
+    const int32_t* int2api = api_is_internal(pg) ? nullptr : pg->old2new.as<int32_t>();
+    if (hashed || int2api) {
+        prio = pg->scratch.take<uint64_t>(n);
+        k_mis_prio<<<nb, kThreads, 0, s>>>(n, int2api, pc_graph_key(seed, PC_GEN_PRIORITY), hashed ? 1 : 0, prio);
+        PC_LAUNCHED();
+    }
+    PC_CUDA(cudaMemsetAsync(state, 0, n * 4, s));
+    // all vertices start undecided
+    k_iota<<<nb, kThreads, 0, s>>>(q0, n);
+    PC_LAUNCHED();
+    uint32_t un = (uint32_t)n;
+    int32_t* fq = q0;
+    int32_t* nq = q1;
+    for (uint64_t round = 0; un > 0; ++round) {
+        PC_CUDA(cudaMemsetAsync(cnt, 0, 4, s));
+        k_mis_round<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, prio, fq, un, state, nq, cnt);
+        PC_LAUNCHED();
+        PC_TRY(read_u32(pg, cnt, &un));
+        std::swap(fq, nq);
+        if (round > n + 1) return fail(PC_ERR_TIMEOUT, "MIS did not converge");
+    }
+    k_mis_finish<<<nb, kThreads, 0, s>>>(state, n, q0);
+    PC_LAUNCHED();
+    PC_TRY(gather_to_api_i32(pg, q0, out));
+    PC_CUDA(cudaMemcpyAsync(res_host, out, n * 4, cudaMemcpyDeviceToHost, s));
+    return sync(pg);
+}
+
+}  // namespace pc
+
+using namespace pc;
+
+extern "C" {
+
+pc_status pc_bfs(pc_pgraph* pg, int32_t src, int32_t* rank) {
+    clear_error();
+    if (!pg || !rank) return fail(PC_ERR_INVALID_INPUT, "null argument");
+    const uint64_t n = pg->g->n;
+    if (src < 0 || (uint64_t)src >= n) return fail(PC_ERR_INVALID_INPUT, "source vertex out of range");
+    PC_TRY(use_device(pg->g));
+    return bfs_run(pg, to_internal_id(pg, src), rank);
+}
+
+pc_status pc_sssp(pc_pgraph* pg, int32_t src, int32_t* dist_host) {
+    clear_error();
+    if (!pg || !dist_host) return fail(PC_ERR_INVALID_INPUT, "null argument");
+    const uint64_t n = pg->g->n;
+    if (!pg->w) return fail(PC_ERR_INVALID_INPUT, "SSSP needs a weighted graph");
+    if (src < 0 || (uint64_t)src >= n) return fail(PC_ERR_INVALID_INPUT, "source vertex out of range");
+    PC_TRY(use_device(pg->g));
+    const int32_t isrc = to_internal_id(pg, src);
+    cudaStream_t s = pg->g->stream;
+    PC_TRY(scratch_reserve(pg, n * 4 * 5 + 256));
+    int32_t* dist = pg->scratch.take<int32_t>(n);
+    int32_t* flag = pg->scratch.take<int32_t>(n);
+    int32_t* q0 = pg->scratch.take<int32_t>(n);
+    int32_t* q1 = pg->scratch.take<int32_t>(n);
+    int32_t* out = pg->scratch.take<int32_t>(n);
+    uint32_t* cnt = pg->scratch.take<uint32_t>(4);
+    const unsigned nb = (unsigned)ceil_div(n, kThreads);
+    k_fill_i32<<<nb, kThreads, 0, s>>>(dist, n, INT_MAX / 2);  // src/test.cpp:202-203
+    PC_LAUNCHED();
+    PC_CUDA(cudaMemsetAsync(flag, 0, n * 4, s));
+    const int32_t zero = 0;
+    PC_CUDA(cudaMemcpyAsync(dist + isrc, &zero, 4, cudaMemcpyHostToDevice, s));
+    PC_CUDA(cudaMemcpyAsync(q0, &isrc, 4, cudaMemcpyHostToDevice, s));
+    uint32_t fn = 1;
+    int32_t* fq = q0;
+    int32_t* nq = q1;
+    for (uint64_t round = 0; fn > 0; ++round) {
+        PC_CUDA(cudaMemsetAsync(cnt, 0, 4, s));
+        k_sssp_relax<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, pg->w, fq, fn, dist, flag, nq, cnt);
+        PC_LAUNCHED();
+        PC_TRY(read_u32(pg, cnt, &fn));
+        if (fn) {
+            k_clear_flags<<<(unsigned)ceil_div(fn, kThreads), kThreads, 0, s>>>(nq, fn, flag);
+            PC_LAUNCHED();
+        }
+        std::swap(fq, nq);
+        if (round > n + 1) return fail(PC_ERR_TIMEOUT, "SSSP did not converge");
+    }
+    PC_TRY(gather_to_api_i32(pg, dist, out));
+    PC_CUDA(cudaMemcpyAsync(dist_host, out, n * 4, cudaMemcpyDeviceToHost, s));
+    return sync(pg);
+}
+
+pc_status pc_pagerank(pc_pgraph* pg, float damping, int32_t iterations, const float* init, float* out) {
+    clear_error();
+    if (!pg || !out) return fail(PC_ERR_INVALID_INPUT, "null argument");
+    if (iterations <= 0) return fail(PC_ERR_INVALID_INPUT, "iterations must be positive");
+    if (!(damping > 0.f && damping <= 1.f)) return fail(PC_ERR_INVALID_INPUT, "damping must be in (0, 1]");
+    PC_TRY(use_device(pg->g));
+    return pagerank_run<float>(pg, damping, iterations, init, out);
+}
+
+pc_status pc_pagerank_f64(pc_pgraph* pg, double damping, int32_t iterations, const double* init, double* out) {
+    clear_error();
+    if (!pg || !out) return fail(PC_ERR_INVALID_INPUT, "null argument");
+    if (iterations <= 0) return fail(PC_ERR_INVALID_INPUT, "iterations must be positive");
+    if (!(damping > 0.0 && damping <= 1.0)) return fail(PC_ERR_INVALID_INPUT, "damping must be in (0, 1]");
+    PC_TRY(use_device(pg->g));
+    return pagerank_run<double>(pg, damping, iterations, init, out);
+}
+
+pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
+    clear_error();
+    if (!pg || !core_host) return fail(PC_ERR_INVALID_INPUT, "null argument");
+    PC_TRY(use_device(pg->g));
+    const uint64_t n = pg->g->n;
+    cudaStream_t s = pg->g->stream;
+    if (n == 0) {
+        if (largest) *largest = 0;
+        return PC_OK;
+    }
+    PC_TRY(scratch_reserve(pg, n * 4 * 7 + 1024));
+    int32_t* deg = pg->scratch.take<int32_t>(n);
+    int32_t* core = pg->scratch.take<int32_t>(n);
+    int32_t* rem = pg->scratch.take<int32_t>(n);
+    int32_t* rem2 = pg->scratch.take<int32_t>(n);
+    int32_t* f0 = pg->scratch.take<int32_t>(n);
+    int32_t* f1 = pg->scratch.take<int32_t>(n);
+    int32_t* out = pg->scratch.take<int32_t>(n);
+    uint32_t* cnt = pg->scratch.take<uint32_t>(4);  // 0 frontier, 1 remaining, 2 next frontier
+    int32_t* minleft = pg->scratch.take<int32_t>(1);
+    const unsigned nb = (unsigned)ceil_div(n, kThreads);
+    k_kcore_init<<<nb, kThreads, 0, s>>>(pg->off, n, deg, core, rem);
+    PC_LAUNCHED();
+    uint32_t rn = (uint32_t)n;
+    int32_t k = 1, top = 0;
+    // Levels k = 1 .. n-1, as the reference's loop (src/Graph.cpp:683, 1893);
+    // vertices never peeled (only in a complete graph) keep core 0.
+    while (rn > 0 && (uint64_t)k < n) {
+        // level k: peel every remaining vertex of degree < k (src/Graph.cpp:683-717)
+        PC_CUDA(cudaMemsetAsync(cnt, 0, 16, s));
+        const int32_t big = INT_MAX;
+        PC_CUDA(cudaMemcpyAsync(minleft, &big, 4, cudaMemcpyHostToDevice, s));
+        k_kcore_scan<<<(unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(rn, kThreads), grid_for(pg, 16))),
+                       kThreads, 0, s>>>(rem, rn, k, deg, core, f0, cnt, rem2, cnt + 1, minleft);
+        PC_LAUNCHED();
+        uint32_t h[2];
+        int32_t ml = 0;
+        PC_CUDA(cudaMemcpyAsync(h, cnt, 8, cudaMemcpyDeviceToHost, s));
+        PC_CUDA(cudaMemcpyAsync(&ml, minleft, 4, cudaMemcpyDeviceToHost, s));
+        PC_CUDA(cudaStreamSynchronize(s));
+        uint32_t fn = h[0];
+        std::swap(rem, rem2);
+        rn = h[1];
+        if (fn == 0) {
+            // Nothing below k: every remaining degree is >= ml (read with no
+            // peeling in flight), so levels k..ml are empty; the reference
+            // makes the same jump (src/Graph.cpp:1921).
+            if (rn == 0) break;
+            k = (int32_t)std::min<int64_t>(std::max<int64_t>((int64_t)k + 1, (int64_t)ml + 1), (int64_t)n);
+            continue;
+        }
+        top = k - 1;
+        int32_t* fq = f0;
+        int32_t* nq = f1;
+        while (fn > 0) {
+            PC_CUDA(cudaMemsetAsync(cnt + 2, 0, 4, s));
+            k_kcore_peel<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, fq, fn, k, deg, core, nq, cnt + 2);
+            PC_LAUNCHED();
+            PC_TRY(read_u32(pg, cnt + 2, &fn));
+            std::swap(fq, nq);
+        }
+        // peeling may have pushed kept vertices down to exactly k: rescan at k+1
+        ++k;
+    }
+    k_kcore_unpeeled<<<nb, kThreads, 0, s>>>(core, n);
+    PC_LAUNCHED();
+    // vertices kept in `rem` may have been peeled after the scan: all have core >= 0 now
+    PC_TRY(gather_to_api_i32(pg, core, out));
+    PC_CUDA(cudaMemcpyAsync(core_host, out, n * 4, cudaMemcpyDeviceToHost, s));
+    PC_TRY(sync(pg));
+    if (largest) *largest = top;
+    return PC_OK;
+}
+
+pc_status pc_mis(pc_pgraph* pg, int32_t* res) {
+    clear_error();
+    if (!pg || !res) return fail(PC_ERR_INVALID_INPUT, "null argument");
+    PC_TRY(use_device(pg->g));
+    if (pg->g->n == 0) return PC_OK;
+    return mis_run(pg, false, 0, res);
+}
+
+pc_status pc_mis_hashed(pc_pgraph* pg, uint64_t seed, int32_t* res) {
+    clear_error();
+    if (!pg || !res) return fail(PC_ERR_INVALID_INPUT, "null argument");
+    PC_TRY(use_device(pg->g));
+    if (pg->g->n == 0) return PC_OK;
+    return mis_run(pg, true, seed, res);
+}
+
+pc_status pc_cdlp(pc_pgraph* pg, int32_t iterations, int32_t* labels) {
+    clear_error();
+    if (!pg || !labels) return fail(PC_ERR_INVALID_INPUT, "null argument");
+    if (iterations < 0) return fail(PC_ERR_INVALID_INPUT, "iterations must be non-negative");
+    PC_TRY(use_device(pg->g));
+    const uint64_t n = pg->g->n;
+    if (n == 0 || iterations == 0) return PC_OK;
+    cudaStream_t s = pg->g->stream;
+    PC_TRY(scratch_reserve(pg, n * 4 * 3 + 256));
+    int32_t* a = pg->scratch.take<int32_t>(n);
+    int32_t* b = pg->scratch.take<int32_t>(n);
+    int32_t* c = pg->scratch.take<int32_t>(n);
+    PC_CUDA(cudaMemcpyAsync(c, labels, n * 4, cudaMemcpyHostToDevice, s));
+    PC_TRY(gather_to_internal_i32(pg, c, a));
+    for (int32_t it = 0; it < iterations; ++it) {
+        k_cdlp_iter<<<grid_for(pg, 16), kThreads, 0, s>>>(pg->off, pg->adj, n, a, b);
+        PC_LAUNCHED();
+        std::swap(a, b);
+    }
+    PC_TRY(gather_to_api_i32(pg, a, c));
+    PC_CUDA(cudaMemcpyAsync(labels, c, n * 4, cudaMemcpyDeviceToHost, s));
+    return sync(pg);
+}
+
+}  // extern "C"

@@ -6,6 +6,7 @@
 #include <string>
 
 #include "../../../include/pc.h"
+#include "../synth_rng.h"
 #include "host_csr.hpp"
 
 namespace pc {
@@ -118,6 +119,14 @@ pc_status pc_host_csr_from_arrays(const uint64_t* vlist, const int32_t* elist, c
 pc_status pc_host_csr_free(pc_host_csr* g) {
     pc::clear_error();
     delete g;
+    return PC_OK;
+}
+
+pc_status pc_synth_vertex_priority(uint64_t seed, uint64_t n, uint64_t* out) {
+    pc::clear_error();
+    if (n && !out) return fail(PC_ERR_INVALID_INPUT, "null output");
+    const uint64_t key = pc_graph_key(seed, PC_GEN_PRIORITY);
+    for (uint64_t v = 0; v < n; ++v) out[v] = pc_vertex_priority(key, (uint32_t)v);
     return PC_OK;
 }
 

@@ -1,0 +1,416 @@
+// Per-edge common-neighbour counts (LCC, all-edge Jaccard), Jaccard over a
+// query list, and batched pair / k-set intersection counts (sm_100a).
+//
+// Per-edge counts c({u,v}) = |N(u) & N(v)| are built by listing every
+// triangle once in the pivot form of the TC kernels (a < b < c found at pivot
+// b from in-neighbour c) and adding 1 to its three edges.  An undirected edge
+// {x, y}, y < x, is counted at its oriented slot: position k of y in row x
+// (k < dplus[x]).  A finalisation pass reads, for every CSR entry, its own
+// slot or its twin's, and forms the Jaccard ratio and the LCC numerator
+// sum_{v in N(u)} c({u,v}) exactly as the reference defines them
+// (src/Graph.cpp:798-840).
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+
+#include "pc_internal.cuh"
+
+namespace pc {
+namespace ix {
+
+constexpr int kThreads = 512;
+constexpr int kChunk = 2048;     // in-neighbours per work item
+constexpr int kMapSlots = 4096;  // pivot map: open addressing
+constexpr int kMapCap = 2048;    // pivots with a larger set take the global path
+
+struct Item {
+    int32_t b;
+    int32_t j0;
+};
+
+__device__ __forceinline__ uint32_t map_slot(int32_t a) { return ((uint32_t)a * 0x9E3779B1u) >> (32 - 12); }
+
+// lower_bound of x in sorted p[0..n)
+__device__ __forceinline__ uint32_t lb(const int32_t* __restrict__ p, uint32_t n, int32_t x) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (p[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_items_count(const uint64_t* __restrict__ off, const uint32_t* __restrict__ dplus, uint64_t n,
+                              uint32_t* __restrict__ cnt) {
+    const uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (b > n) return;
+    if (b == n) { cnt[b] = 0; return; }
+    const uint32_t dp = dplus[b];
+    const uint64_t din = off[b + 1] - off[b] - dp;
+    cnt[b] = (dp == 0 || din == 0) ? 0u : (uint32_t)((din + kChunk - 1) / kChunk);
+}
+
+__global__ void k_items_fill(const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ start, uint64_t n,
+                             Item* __restrict__ items) {
+    const uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    const uint32_t c = cnt[b], s = start[b];
+    for (uint32_t j = 0; j < c; ++j) items[s + j] = Item{(int32_t)b, (int32_t)(j * kChunk)};
+}
+
+// Triangle listing with per-edge increments (one CTA per work item; warps
+// scan in-neighbour prefixes 32 ids at a time).
+__global__ void __launch_bounds__(kThreads) k_edge_counts(const uint64_t* __restrict__ off,
+                                                          const int32_t* __restrict__ adj,
+                                                          const uint32_t* __restrict__ dplus,
+                                                          const Item* __restrict__ items,
+                                                          const uint32_t* __restrict__ nitems_p,
+                                                          uint32_t* __restrict__ next_item,
+                                                          uint32_t* __restrict__ ecnt) {
+    extern __shared__ int32_t smap[];  // key | idx | hit, kMapSlots each
+    int32_t* key = smap;
+    uint32_t* idx = reinterpret_cast<uint32_t*>(smap + kMapSlots);
+    uint32_t* hit = reinterpret_cast<uint32_t*>(smap + 2 * kMapSlots);
+    __shared__ uint32_t s_item;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    for (int i = tid; i < kMapSlots; i += blockDim.x) { key[i] = -1; hit[i] = 0; }
+    const uint32_t nitems = *nitems_p;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(next_item, 1u);
+        __syncthreads();
+        const uint32_t it = s_item;
+        if (it >= nitems) break;
+        const Item I = items[it];
+        const int32_t b = I.b;
+        const uint64_t rb = off[b], re = off[b + 1];
+        const uint32_t dp = dplus[b];
+        const bool use_map = dp <= (uint32_t)kMapCap;
+        if (use_map) {
+            for (uint32_t k = tid; k < dp; k += blockDim.x) {
+                const int32_t a = adj[rb + k];
+                uint32_t s = map_slot(a);
+                while (atomicCAS(&key[s], -1, a) != -1) s = (s + 1) & (kMapSlots - 1);
+                idx[s] = k;
+            }
+        }
+        __syncthreads();
+        const uint64_t in0 = rb + dp + (uint64_t)I.j0;
+        const uint64_t in1 = min(in0 + (uint64_t)kChunk, re);
+        for (uint64_t e = in0 + warp; e < in1; e += nw) {
+            const int32_t c = adj[e];
+            const uint64_t rc = off[c];
+            const uint32_t lim = dplus[c];
+            uint32_t pair_hits = 0, kb = 0xffffffffu;
+            for (uint32_t i0 = 0; i0 < lim; i0 += 32) {
+                const uint32_t i = i0 + lane;
+                const int32_t a = i < lim ? __ldg(adj + rc + i) : 0x7fffffff;
+                if (a < b) {
+                    bool found = false;
+                    if (use_map) {
+                        uint32_t s = map_slot(a);
+                        int32_t kk;
+                        while ((kk = key[s]) != -1) {
+                            if (kk == a) { found = true; atomicAdd(&hit[s], 1u); break; }
+                            s = (s + 1) & (kMapSlots - 1);
+                        }
+                    } else {
+                        const uint32_t p = lb(adj + rb, dp, a);
+                        if (p < dp && adj[rb + p] == a) { found = true; atomicAdd(&ecnt[rb + p], 1u); }
+                    }
+                    if (found) {
+                        ++pair_hits;
+                        atomicAdd(&ecnt[rc + i], 1u);  // edge {c, a}
+                    }
+                }
+                const unsigned at_b = __ballot_sync(0xffffffffu, a == b);
+                if (at_b) kb = i0 + __ffs(at_b) - 1;
+                const int32_t last = __shfl_sync(0xffffffffu, a, 31);
+                if (last >= b) break;
+            }
+            for (int o = 16; o; o >>= 1) pair_hits += __shfl_xor_sync(0xffffffffu, pair_hits, o);
+            if (lane == 0 && pair_hits && kb != 0xffffffffu) atomicAdd(&ecnt[rc + kb], pair_hits);  // edge {c, b}
+        }
+        __syncthreads();
+        if (use_map) {
+            for (int s = tid; s < kMapSlots; s += blockDim.x) {
+                if (key[s] != -1) {
+                    if (hit[s]) atomicAdd(&ecnt[rb + idx[s]], hit[s]);  // edges {b, a}
+                    key[s] = -1;
+                    hit[s] = 0;
+                }
+            }
+        }
+    }
+}
+
+// Count of the undirected edge behind CSR entry (u, v) at position e.
+__device__ __forceinline__ uint32_t edge_count(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                                               const uint32_t* __restrict__ dplus, const uint32_t* __restrict__ ecnt,
+                                               uint64_t u, int32_t v, uint64_t e) {
+    if ((uint64_t)v < u) return ecnt[e];
+    const uint64_t rv = off[v];
+    return ecnt[rv + lb(adj + rv, dplus[v], (int32_t)u)];
+}
+
+// Jaccard per entry (fp32 output of the fp64 formula) and LCC per row.
+__global__ void k_finalize(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                           const uint32_t* __restrict__ dplus, const uint32_t* __restrict__ ecnt, uint64_t n,
+                           float* __restrict__ jac, double* __restrict__ lcc) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t u = warp; u < n; u += nwarps) {
+        const uint64_t b = off[u], e = off[u + 1];
+        const uint64_t du = e - b;
+        unsigned long long sum = 0;
+        for (uint64_t j = b + lane; j < e; j += 32) {
+            const int32_t v = adj[j];
+            const uint32_t c = edge_count(off, adj, dplus, ecnt, u, v, j);
+            sum += c;
+            if (jac) {
+                const uint64_t dv = off[v + 1] - off[v];
+                // src/Graph.cpp:808-809: c / (deg_u + deg_v - c), in double
+                jac[j] = (float)((double)c / ((double)(du + dv) - (double)c));
+            }
+        }
+        for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lcc && lane == 0) {
+            // src/Graph.cpp:833-838: d = 0 -> 0; else sum / (d (d - 1)) (d = 1 gives 0/0)
+            lcc[u] = du < 1 ? 0.0 : (double)sum / (double)(du * (du - 1));
+        }
+    }
+}
+
+// |N(a) & N(b)| for each pair: lanes take ids of the shorter list and look
+// them up in the longer one by binary search (galloping probing).
+__global__ void k_pair_counts(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                              const int32_t* __restrict__ pairs, uint64_t nq, unsigned long long* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t q = warp; q < nq; q += nwarps) {
+        int32_t a = pairs[2 * q], b = pairs[2 * q + 1];
+        uint64_t ra = off[a], la = off[a + 1] - ra, rb = off[b], lb_ = off[b + 1] - rb;
+        if (la > lb_) { uint64_t t = ra; ra = rb; rb = t; t = la; la = lb_; lb_ = t; }
+        unsigned long long c = 0;
+        for (uint64_t i = lane; i < la; i += 32) {
+            const int32_t x = adj[ra + i];
+            const uint32_t p = lb(adj + rb, (uint32_t)lb_, x);
+            c += (p < lb_ && adj[rb + p] == x) ? 1 : 0;
+        }
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0) out[q] = c;
+    }
+}
+
+// |AND_j N(s_j)| for each k-set: ids of the shortest list looked up in all others.
+__global__ void k_set_counts(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                             const int32_t* __restrict__ ids, const uint64_t* __restrict__ soff, uint64_t nq,
+                             unsigned long long* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t q = warp; q < nq; q += nwarps) {
+        const uint64_t s0 = soff[q], s1 = soff[q + 1];
+        // shortest list
+        uint64_t best = s0, bestlen = ~0ull;
+        for (uint64_t t = s0; t < s1; ++t) {
+            const int32_t v = ids[t];
+            const uint64_t l = off[v + 1] - off[v];
+            if (l < bestlen) { bestlen = l; best = t; }
+        }
+        const int32_t sv = ids[best];
+        const uint64_t rs = off[sv];
+        unsigned long long c = 0;
+        for (uint64_t i = lane; i < bestlen; i += 32) {
+            const int32_t x = adj[rs + i];
+            bool all = true;
+            for (uint64_t t = s0; t < s1 && all; ++t) {
+                if (t == best) continue;
+                const int32_t v = ids[t];
+                const uint64_t rv = off[v], lv = off[v + 1] - rv;
+                const uint32_t p = lb(adj + rv, (uint32_t)lv, x);
+                all = p < lv && adj[rv + p] == x;
+            }
+            c += all ? 1 : 0;
+        }
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0) out[q] = c;
+    }
+}
+
+__global__ void k_jaccard_pairs(const uint64_t* __restrict__ off, const int32_t* __restrict__ q, int32_t nq,
+                                const unsigned long long* __restrict__ c, double* __restrict__ out) {
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t >= (uint64_t)nq * nq) return;
+    const int32_t i = (int32_t)(t / nq), j = (int32_t)(t % nq);
+    const uint64_t du = off[q[i] + 1] - off[q[i]], dv = off[q[j] + 1] - off[q[j]];
+    const double cc = (double)c[t];
+    out[t] = cc / ((double)(du + dv) - cc);  // src/Graph.cpp:808-809
+}
+
+__global__ void k_make_pairs(const int32_t* __restrict__ q, int32_t nq, int32_t* __restrict__ pairs) {
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t >= (uint64_t)nq * nq) return;
+    pairs[2 * t] = q[t / nq];
+    pairs[2 * t + 1] = q[t % nq];
+}
+
+}  // namespace ix
+
+using namespace ix;
+
+// Per-edge counts into a scratch array; returns it.
+static pc_status edge_counts(pc_pgraph* pg, uint32_t** ecnt_out, size_t extra_bytes) {
+    PC_TRY(ensure_dplus(pg));
+    const uint64_t n = pg->g->n, m = pg->g->m;
+    cudaStream_t s = pg->g->stream;
+    size_t tmpb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmpb, (uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t)(n + 1), s);
+    const uint64_t item_bound = n + m / kChunk + 2;
+    PC_TRY(scratch_reserve(pg, m * 4 + (n + 1) * 8 + tmpb + item_bound * sizeof(Item) + 64 + extra_bytes));
+    uint32_t* ecnt = pg->scratch.take<uint32_t>(std::max<uint64_t>(m, 1));
+    uint32_t* cnt = pg->scratch.take<uint32_t>(n + 1);
+    uint32_t* start = pg->scratch.take<uint32_t>(n + 1);
+    void* tmp = pg->scratch.take<char>(tmpb);
+    Item* items = pg->scratch.take<Item>(item_bound);
+    uint32_t* next = pg->scratch.take<uint32_t>(1);
+    if (!ecnt || !cnt || !start || !tmp || !items || !next) return fail(PC_ERR_OOM, "scratch sizing error");
+    PC_CUDA(cudaMemsetAsync(ecnt, 0, std::max<uint64_t>(m, 1) * 4, s));
+    PC_CUDA(cudaMemsetAsync(next, 0, 4, s));
+    const uint32_t* dp = pg->dplus.as<uint32_t>();
+    k_items_count<<<(unsigned)ceil_div(n + 1, 256), 256, 0, s>>>(pg->off, dp, n, cnt);
+    PC_LAUNCHED();
+    PC_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmpb, cnt, start, (int64_t)(n + 1), s));
+    count_launch();
+    k_items_fill<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(cnt, start, n, items);
+    PC_LAUNCHED();
+    const int sms = sm_count(pg->g->device);
+    const int smem = kMapSlots * 12;
+    PC_CUDA(cudaFuncSetAttribute(k_edge_counts, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_edge_counts<<<sms * 2, kThreads, smem, s>>>(pg->off, pg->adj, dp, items, start + n, next, ecnt);
+    PC_LAUNCHED();
+    *ecnt_out = ecnt;
+    return PC_OK;
+}
+
+}  // namespace pc
+
+using namespace pc;
+
+extern "C" {
+
+pc_status pc_lcc(pc_pgraph* pg, int32_t method, double* out) {
+    clear_error();
+    if (!pg || !out) return fail(PC_ERR_INVALID_INPUT, "null argument");
+    if (method != PC_METHOD_MERGE && method != PC_METHOD_GALLOPING) return fail(PC_ERR_INVALID_INPUT, "unknown method");
+    PC_TRY(use_device(pg->g));
+    const uint64_t n = pg->g->n;
+    if (n == 0) return PC_OK;
+    uint32_t* ecnt = nullptr;
+    PC_TRY(edge_counts(pg, &ecnt, n * 8 * 2 + 512));
+    double* lcc = pg->scratch.take<double>(n);
+    double* lcc_api = pg->scratch.take<double>(n);
+    cudaStream_t s = pg->g->stream;
+    k_finalize<<<sm_count(pg->g->device) * 16, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), ecnt, n,
+                                                             nullptr, lcc);
+    PC_LAUNCHED();
+    PC_TRY(gather_to_api_f64(pg, lcc, lcc_api));
+    PC_CUDA(cudaMemcpyAsync(out, lcc_api, n * 8, cudaMemcpyDeviceToHost, s));
+    return sync(pg);
+}
+
+pc_status pc_jaccard_edges(pc_pgraph* pg, float* out) {
+    clear_error();
+    if (!pg || !out) return fail(PC_ERR_INVALID_INPUT, "null argument");
+    PC_TRY(use_device(pg->g));
+    const uint64_t n = pg->g->n, m = pg->g->m;
+    if (m == 0) return PC_OK;
+    uint32_t* ecnt = nullptr;
+    PC_TRY(edge_counts(pg, &ecnt, m * 4 + 512));
+    float* jac = pg->scratch.take<float>(m);
+    cudaStream_t s = pg->g->stream;
+    k_finalize<<<sm_count(pg->g->device) * 16, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), ecnt, n,
+                                                             jac, nullptr);
+    PC_LAUNCHED();
+    // entries are in the graph's own CSR order (internal ids are the graph's ids)
+    PC_CUDA(cudaMemcpyAsync(out, jac, m * 4, cudaMemcpyDeviceToHost, s));
+    return sync(pg);
+}
+
+pc_status pc_batch_count_pairs(pc_pgraph* pg, const int32_t* pairs, uint64_t nq, uint64_t* out) {
+    clear_error();
+    if (!pg || (nq && (!pairs || !out))) return fail(PC_ERR_INVALID_INPUT, "null argument");
+    if (nq == 0) return PC_OK;
+    const uint64_t n = pg->g->n;
+    for (uint64_t i = 0; i < 2 * nq; ++i)
+        if (pairs[i] < 0 || (uint64_t)pairs[i] >= n) return fail(PC_ERR_INVALID_INPUT, "query vertex out of range");
+    PC_TRY(use_device(pg->g));
+    cudaStream_t s = pg->g->stream;
+    PC_TRY(scratch_reserve(pg, nq * 8 + nq * 8 + 512));
+    int32_t* d_pairs = nullptr;
+    PC_TRY(upload(pg, pairs, 2 * nq, &d_pairs));
+    PC_TRY(map_ids_to_internal(pg, d_pairs, 2 * nq));
+    unsigned long long* d_out = pg->scratch.take<unsigned long long>(nq);
+    k_pair_counts<<<sm_count(pg->g->device) * 16, 256, 0, s>>>(pg->off, pg->adj, d_pairs, nq, d_out);
+    PC_LAUNCHED();
+    PC_CUDA(cudaMemcpyAsync(out, d_out, nq * 8, cudaMemcpyDeviceToHost, s));
+    return sync(pg);
+}
+
+pc_status pc_batch_count_sets(pc_pgraph* pg, const int32_t* ids, const uint64_t* offsets, uint64_t nq, uint64_t* out) {
+    clear_error();
+    if (!pg || (nq && (!ids || !offsets || !out))) return fail(PC_ERR_INVALID_INPUT, "null argument");
+    if (nq == 0) return PC_OK;
+    const uint64_t n = pg->g->n;
+    if (offsets[0] != 0) return fail(PC_ERR_INVALID_INPUT, "offsets[0] must be 0");
+    for (uint64_t i = 0; i < nq; ++i)
+        if (offsets[i + 1] <= offsets[i]) return fail(PC_ERR_INVALID_INPUT, "every set needs at least one vertex");
+    const uint64_t tot = offsets[nq];
+    for (uint64_t i = 0; i < tot; ++i)
+        if (ids[i] < 0 || (uint64_t)ids[i] >= n) return fail(PC_ERR_INVALID_INPUT, "query vertex out of range");
+    PC_TRY(use_device(pg->g));
+    cudaStream_t s = pg->g->stream;
+    PC_TRY(scratch_reserve(pg, tot * 4 + (nq + 1) * 8 + nq * 8 + 512));
+    int32_t* d_ids = nullptr;
+    uint64_t* d_off = nullptr;
+    PC_TRY(upload(pg, ids, tot, &d_ids));
+    PC_TRY(upload(pg, offsets, nq + 1, &d_off));
+    PC_TRY(map_ids_to_internal(pg, d_ids, tot));
+    unsigned long long* d_out = pg->scratch.take<unsigned long long>(nq);
+    k_set_counts<<<sm_count(pg->g->device) * 16, 256, 0, s>>>(pg->off, pg->adj, d_ids, d_off, nq, d_out);
+    PC_LAUNCHED();
+    PC_CUDA(cudaMemcpyAsync(out, d_out, nq * 8, cudaMemcpyDeviceToHost, s));
+    return sync(pg);
+}
+
+pc_status pc_jaccard_queries(pc_pgraph* pg, const int32_t* queries, int32_t nq, double* out) {
+    clear_error();
+    if (!pg || nq < 0 || (nq && (!queries || !out))) return fail(PC_ERR_INVALID_INPUT, "bad argument");
+    if (nq == 0) return PC_OK;
+    const uint64_t n = pg->g->n;
+    for (int32_t i = 0; i < nq; ++i)
+        if (queries[i] < 0 || (uint64_t)queries[i] >= n) return fail(PC_ERR_INVALID_INPUT, "query vertex out of range");
+    PC_TRY(use_device(pg->g));
+    cudaStream_t s = pg->g->stream;
+    const uint64_t np = (uint64_t)nq * nq;
+    PC_TRY(scratch_reserve(pg, nq * 4 + np * 8 + np * 8 + np * 8 + 512));
+    int32_t* d_q = nullptr;
+    PC_TRY(upload(pg, queries, (size_t)nq, &d_q));
+    PC_TRY(map_ids_to_internal(pg, d_q, nq));
+    int32_t* d_pairs = pg->scratch.take<int32_t>(2 * np);
+    unsigned long long* d_c = pg->scratch.take<unsigned long long>(np);
+    double* d_out = pg->scratch.take<double>(np);
+    k_make_pairs<<<(unsigned)ceil_div(np, 256), 256, 0, s>>>(d_q, nq, d_pairs);
+    PC_LAUNCHED();
+    k_pair_counts<<<sm_count(pg->g->device) * 16, 256, 0, s>>>(pg->off, pg->adj, d_pairs, np, d_c);
+    PC_LAUNCHED();
+    k_jaccard_pairs<<<(unsigned)ceil_div(np, 256), 256, 0, s>>>(pg->off, d_q, nq, d_c, d_out);
+    PC_LAUNCHED();
+    PC_CUDA(cudaMemcpyAsync(out, d_out, np * 8, cudaMemcpyDeviceToHost, s));
+    return sync(pg);
+}
+
+}  // extern "C"

@@ -146,6 +146,12 @@ pc_status gather_to_api_i32(pc_pgraph* pg, const int32_t* in_internal, int32_t* 
 pc_status gather_to_api_f32(pc_pgraph* pg, const float* in_internal, float* out_api);
 pc_status gather_to_api_f64(pc_pgraph* pg, const double* in_internal, double* out_api);
 bool api_is_internal(const pc_pgraph* pg);
+// out_internal[u] = in_api[API id of u] (a gather by old2new).
+pc_status gather_to_internal_i32(pc_pgraph* pg, const int32_t* in_api, int32_t* out_internal);
+pc_status gather_to_internal_f32(pc_pgraph* pg, const float* in_api, float* out_internal);
+pc_status gather_to_internal_f64(pc_pgraph* pg, const double* in_api, double* out_internal);
+// Internal id of one API vertex id (synchronous).
+int32_t to_internal_id(const pc_pgraph* pg, int32_t api_id);
 
 // Lazily computes pg->dplus.
 pc_status ensure_dplus(pc_pgraph* pg);

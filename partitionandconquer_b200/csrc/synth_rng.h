@@ -76,7 +76,9 @@ PC_HD int32_t pc_edge_weight(uint64_t key, uint32_t a, uint32_t b, int32_t wmax)
     return 1 + (int32_t)(((x >> 32) * (uint64_t)wmax) >> 32);
 }
 
-// Seed-hashed vertex priority (used to relabel vertices for the MIS order).
+// Seed-hashed vertex priority for the MIS order: the top 33 bits of
+// draw(key, v) above the 31-bit id, so priorities are distinct and ties can
+// never occur.
 PC_HD uint64_t pc_vertex_priority(uint64_t key, uint32_t v) {
-    return pc_draw(key, v);
+    return ((pc_draw(key, v) >> 31) << 31) | (uint64_t)(v & 0x7FFFFFFFu);
 }

@@ -1,0 +1,139 @@
+"""The learned per-partition selector: the MLP's hand-written GPU forward and
+backward kernels against an FP64 CPU restatement (gradient check), training,
+and the selector end to end (collect timings, train, plan) -- with exact
+triangle counts whatever the plan."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+IN, H, OUT = 12, 64, 6
+
+
+def unpack(p):
+    p = np.asarray(p, np.float64)
+    o = 0
+    W1 = p[o:o + H * IN].reshape(H, IN); o += H * IN
+    b1 = p[o:o + H]; o += H
+    W2 = p[o:o + H * H].reshape(H, H); o += H * H
+    b2 = p[o:o + H]; o += H
+    W3 = p[o:o + OUT * H].reshape(OUT, H); o += OUT * H
+    b3 = p[o:o + OUT]; o += OUT
+    assert o == p.size
+    return W1, b1, W2, b2, W3, b3
+
+
+def cpu_loss_grad(p, x, y, m):
+    """FP64 forward/backward of the same network and masked MSE loss."""
+    W1, b1, W2, b2, W3, b3 = unpack(p)
+    x = x.astype(np.float64); y = y.astype(np.float64); m = m.astype(np.float64)
+    z1 = x @ W1.T + b1; h1 = np.maximum(z1, 0)
+    z2 = h1 @ W2.T + b2; h2 = np.maximum(z2, 0)
+    out = h2 @ W3.T + b3
+    cnt = m.sum()
+    d = (out - y) * m
+    loss = (d * d).sum() / cnt
+    dy = 2 * d / cnt
+    gW3 = dy.T @ h2; gb3 = dy.sum(0)
+    dh2 = (dy @ W3) * (z2 > 0)
+    gW2 = dh2.T @ h1; gb2 = dh2.sum(0)
+    dh1 = (dh2 @ W2) * (z1 > 0)
+    gW1 = dh1.T @ x; gb1 = dh1.sum(0)
+    g = np.concatenate([gW1.ravel(), gb1, gW2.ravel(), gb2, gW3.ravel(), gb3])
+    return loss, g, out
+
+
+def random_problem(seed, batch=53):
+    rng = np.random.default_rng(seed)
+    p = (rng.standard_normal(IN * H + H + H * H + H + OUT * H + OUT) * 0.2).astype(np.float32)
+    x = rng.standard_normal((batch, IN)).astype(np.float32)
+    y = rng.standard_normal((batch, OUT)).astype(np.float32)
+    m = (rng.random((batch, OUT)) < 0.7).astype(np.uint8)
+    return p, x, y, m
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_mlp_gradient_matches_fp64_cpu(gpu, seed):
+    sel = gpu.selector
+    p, x, y, m = random_problem(seed)
+    assert sel.mlp_num_params() == p.size
+    loss, grad = sel.mlp_loss_grad(p, x, y, m)
+    ref_loss, ref_grad, ref_out = cpu_loss_grad(p, x, y, m)
+    np.testing.assert_allclose(sel.mlp_forward(p, x), ref_out, rtol=1e-4, atol=1e-5)
+    assert loss == pytest.approx(ref_loss, rel=1e-4)
+    scale = np.abs(ref_grad).max()
+    np.testing.assert_allclose(grad, ref_grad, rtol=1e-3, atol=1e-5 * scale)
+
+
+def test_mlp_gradient_finite_differences(gpu):
+    sel = gpu.selector
+    p, x, y, m = random_problem(7, batch=16)
+    _, grad = sel.mlp_loss_grad(p, x, y, m)
+    rng = np.random.default_rng(3)
+    p64 = p.astype(np.float64)
+    for i in rng.choice(p.size, 12, replace=False):
+        e = np.zeros_like(p64); e[i] = 1e-5
+        lp, _, _ = cpu_loss_grad(p64 + e, x, y, m)
+        lm, _, _ = cpu_loss_grad(p64 - e, x, y, m)
+        fd = (lp - lm) / 2e-5
+        assert grad[i] == pytest.approx(fd, rel=2e-2, abs=2e-5), i
+
+
+def test_mlp_training_reduces_loss(gpu):
+    sel = gpu.selector
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal((200, IN)).astype(np.float32)
+    w = rng.standard_normal((IN, OUT))
+    y = np.tanh(x @ w).astype(np.float32)
+    m = np.ones((200, OUT), np.uint8)
+    p = (rng.standard_normal(sel.mlp_num_params()) * 0.1).astype(np.float32)
+    l0, _ = sel.mlp_loss_grad(p, x, y, m)
+    p2, l1 = sel.mlp_train_steps(p, x, y, m, 300, 3e-3)
+    assert l1 < 0.25 * l0
+    l2, _ = sel.mlp_loss_grad(p2, x, y, m)
+    assert l2 == pytest.approx(l1, rel=0.2)
+
+
+def test_selector_end_to_end_exact(gpu, O, tmp_path):
+    pc = gpu
+    sel = pc.selector
+    sel.clear()
+    graphs = [pc.HostCSR.rmat(14, 16, 3), pc.HostCSR.er(14, 1 << 18, 4), pc.HostCSR.chung_lu(14, 1 << 18, 2.1, 2048, 5)]
+    pgs = []
+    for h in graphs:
+        vl, el, _ = h.arrays()
+        n = vl.size - 1
+        pg = pc.Partitioned_Graph(pc.Graph(vlist=vl, elist=el), pc.equal_vertex_partition(n, 16))
+        pgs.append((pg, O.tc_merge(vl, el)))
+        assert sel.collect(pg, max_units=16, repeats=1) > 0
+    f, y, m = sel.samples()
+    assert f.shape[1] == 10 and y.shape[1] == 6 and m.any(axis=1).all()
+    loss = sel.train(steps=400, lr=3e-3, seed=5)
+    assert np.isfinite(loss)
+    assert sel.trained()
+    pred = sel.predict(f)
+    assert pred.shape == y.shape and np.isfinite(pred).all()
+    tuned = sel.autotune()
+    assert tuned.shape == (3,)
+    for pg, t in pgs:
+        assert pg.triangle_count(variant=pc.VARIANT_AUTO) == t
+        c, st = pg.triangle_count(variant=pc.VARIANT_AUTO, stats=True)
+        assert c == t and st.selector == 2
+        c, st = pg.triangle_count(variant=pc.VARIANT_HEURISTIC, stats=True)
+        assert c == t and st.selector == 1
+        plan = sel.plan(pg, pc.VARIANT_AUTO)
+        assert plan.dtype == np.int8 and plan.max() < 6
+    path = str(tmp_path / "sel.bin")
+    sel.save(path)
+    before = sel.predict(f)
+    sel.clear()
+    assert not sel.trained()
+    sel.load(path)
+    np.testing.assert_allclose(sel.predict(f), before, rtol=1e-6)
+    sel.enable(False)
+    c, st = pgs[0][0].triangle_count(variant=pc.VARIANT_AUTO, stats=True)
+    assert st.selector == 1 and c == pgs[0][1]
+    sel.enable(True)
+    sel.clear()
