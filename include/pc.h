@@ -188,6 +188,26 @@ pc_status pc_mis_hashed(pc_pgraph* pg, uint64_t seed, int32_t* res);
  * label over N(u) (0 for isolated u), iterations times; in/out. */
 pc_status pc_cdlp(pc_pgraph* pg, int32_t iterations, int32_t* labels);
 
+/* ---- allocation-free entry point ------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (their GPU memory belongs to another allocator or pool, or their
+ * path must not risk an allocation's synchronisation or latency): the
+ * triangle count -- each triangle once, as PC_METHOD_MERGE -- of a symmetric
+ * CSR the caller already holds in device memory (d_vlist: n+1 uint64
+ * offsets; d_elist: m int32 ids, rows strictly ascending, no self-loops; the
+ * CSR is not validated).  Nothing is allocated: the temporaries live in a
+ * fixed array inside the library image (about 4 MiB per GPU, held until the
+ * process exits), which caps n at 2^20 vertices; larger graphs return
+ * PC_ERR_INVALID_INPUT.  The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress) with the device current; make that
+ * first call before any stream capture.  Runs on the current device, on
+ * `stream` (NULL: the legacy default stream), and returns once *count is
+ * written.  Every call shares the array, which keeps the previous call's
+ * contents (the counters are cleared at the start of each call): calls that
+ * overlap on the GPU race. */
+pc_status pc_tc_count_noalloc(const uint64_t* d_vlist, const int32_t* d_elist, uint64_t n, uint64_t m,
+                              void* stream, uint64_t* count);
+
 /* ---- per-partition kernel selection (no counterpart in the reference: the
  *      reference runs one scalar merge everywhere) ------------------------- */
 

@@ -98,6 +98,7 @@ _SIG = {
     "pc_mis": (i32, [P, P]),
     "pc_mis_hashed": (i32, [P, u64, P]),
     "pc_cdlp": (i32, [P, i32, P]),
+    "pc_tc_count_noalloc": (i32, [P, P, u64, u64, P, P]),
     "pc_tc_units": (i32, [P, P]),
     "pc_tc_unit_features": (i32, [P, P, i32]),
     "pc_tc_plan": (i32, [P, i32, P, i32]),
