@@ -99,13 +99,12 @@ struct pc_pgraph {
     uint64_t* off = nullptr;
     int32_t* adj = nullptr;
     int32_t* w = nullptr;
-    pc::DevBuf own_off, own_adj, own_w;
     pc::DevBuf old2new, new2old;  // int32 [n] when !contiguous
     pc::DevBuf v2p;               // int32 [n], original ids
     std::vector<int64_t> pstart;  // P+1 partition boundaries (internal ids)
     pc::DevBuf d_pstart;          // int64 [P+1]
     pc::DevBuf dplus;             // uint32 [n]: |N(u) & [0,u)| (internal ids)
-    pc::DevBuf ecount;            // uint32 [n]: reverse-edge helper (lazy)
+    pc::DevBuf unit_of;           // int32 [n]: planning unit of each vertex (tc.cu)
     pc::Scratch scratch;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // planner state (tc.cu)

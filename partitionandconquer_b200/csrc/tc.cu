@@ -29,56 +29,91 @@ static void build_units(const pc_pgraph* pg, std::vector<int64_t>* lo, std::vect
     }
 }
 
-// Per-unit raw statistics (one CTA per unit, one warp per pivot).
-__global__ void k_unit_stats(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
-                             const uint32_t* __restrict__ dplus, const int32_t* __restrict__ plist,
-                             const int64_t* __restrict__ lo, const int64_t* __restrict__ hi,
-                             unsigned long long* __restrict__ out /* kRawStats per unit */) {
-    __shared__ unsigned long long s[kRawStats];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    if (tid < kRawStats) s[tid] = 0;
-    __syncthreads();
+// Unit of every pivot (plist position ranges -> vertex ids).
+__global__ void k_unit_of(const int32_t* __restrict__ plist, const int64_t* __restrict__ lo,
+                          const int64_t* __restrict__ hi, int32_t* __restrict__ unit_of) {
     const int64_t p0 = lo[blockIdx.x], p1 = hi[blockIdx.x];
-    unsigned long long npiv = 0, ein = 0, sdp = 0, mdp = 0, mid = 0, sscan = 0, sld = 0, sld2 = 0, s32 = 0;
-    for (int64_t p = p0 + warp; p < p1; p += nw) {
-        const int32_t b = pivot_at(plist, p);
-        const uint64_t rb = off[b], re = off[b + 1];
-        const uint32_t dp = dplus[b];
-        const uint64_t din = re - rb - dp;
-        if (lane == 0) {
-            npiv += 1;
-            ein += din;
-            sdp += dp;
-            mdp = max(mdp, (unsigned long long)dp);
-            mid = max(mid, (unsigned long long)b + 1);
-            const double ld = log2(1.0 + (double)(re - rb));
-            sld += (unsigned long long)(ld * 1024.0);
-            sld2 += (unsigned long long)(ld * ld * 1024.0);
+    for (int64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) unit_of[pivot_at(plist, p)] = (int32_t)blockIdx.x;
+}
+
+// Per-pivot statistics, one thread per vertex; when a whole warp lies in one
+// unit (the common case: units are runs of positions) it reduces first and
+// lane 0 issues the atomics.
+__global__ void k_unit_pivot_stats(const uint64_t* __restrict__ off, const uint32_t* __restrict__ dplus,
+                                   const int32_t* __restrict__ unit_of, uint64_t n,
+                                   unsigned long long* __restrict__ out /* kRawStats per unit */) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t nr = (n + 31) & ~31ull;
+    const int lane = threadIdx.x & 31;
+    for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < nr; b += stride) {
+        const bool ok = b < n;
+        int32_t u = -1;
+        unsigned long long v[7] = {0, 0, 0, 0, 0, 0, 0};
+        if (ok) {
+            u = unit_of[b];
+            const uint64_t deg = off[b + 1] - off[b];
+            const uint32_t dp = dplus[b];
+            const double ld = log2(1.0 + (double)deg);
+            v[0] = 1;
+            v[1] = deg - dp;
+            v[2] = dp;
+            v[3] = dp;
+            v[4] = b + 1;
+            v[5] = (unsigned long long)(ld * 1024.0);
+            v[6] = (unsigned long long)(ld * ld * 1024.0);
         }
-        if (dp == 0) continue;
-        for (uint64_t e = rb + dp + lane; e < re; e += 32) {
-            const uint32_t dc = dplus[adj[e]];
-            sscan += dc;
-            s32 += dc >= 32 ? 1 : 0;
+        const int32_t u0 = __shfl_sync(0xffffffffu, u, 0);
+        if (__all_sync(0xffffffffu, ok && u == u0)) {
+            for (int o = 16; o; o >>= 1) {
+                v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
+                v[1] += __shfl_xor_sync(0xffffffffu, v[1], o);
+                v[2] += __shfl_xor_sync(0xffffffffu, v[2], o);
+                v[3] = max(v[3], __shfl_xor_sync(0xffffffffu, v[3], o));
+                v[4] = max(v[4], __shfl_xor_sync(0xffffffffu, v[4], o));
+                v[5] += __shfl_xor_sync(0xffffffffu, v[5], o);
+                v[6] += __shfl_xor_sync(0xffffffffu, v[6], o);
+            }
+            if (lane != 0) continue;
+        } else if (!ok) {
+            continue;
+        }
+        unsigned long long* o = out + (uint64_t)u * kRawStats;
+        atomicAdd(&o[0], v[0]);
+        atomicAdd(&o[1], v[1]);
+        atomicAdd(&o[2], v[2]);
+        atomicMax(&o[3], v[3]);
+        atomicMax(&o[4], v[4]);
+        atomicAdd(&o[6], v[5]);
+        atomicAdd(&o[7], v[6]);
+    }
+}
+
+// In-edge statistics: a warp per vertex c streams its prefix N+(c); every
+// pivot b there has c as an in-neighbour and gains dplus[c] (the bound on
+// c's scan).  Lanes hitting the same unit are merged with __match_any_sync,
+// so one atomic per unit and 32 edges.
+__global__ void k_unit_scan_stats(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                                  const uint32_t* __restrict__ dplus, const int32_t* __restrict__ unit_of,
+                                  uint64_t n, unsigned long long* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t c = warp; c < n; c += nwarps) {
+        const uint32_t dc = dplus[c];
+        if (dc == 0) continue;
+        const int32_t* row = adj + off[c];
+        for (uint32_t k0 = 0; k0 < dc; k0 += 32) {
+            const uint32_t k = k0 + lane;
+            const bool ok = k < dc;
+            const int32_t u = ok ? unit_of[row[k]] : -1;
+            const unsigned peers = __match_any_sync(0xffffffffu, u);
+            if (ok && lane == __ffs(peers) - 1) {
+                const unsigned long long cntp = (unsigned long long)__popc(peers);
+                atomicAdd(&out[(uint64_t)u * kRawStats + 5], cntp * dc);
+                if (dc >= 32) atomicAdd(&out[(uint64_t)u * kRawStats + 8], cntp);
+            }
         }
     }
-    for (int o = 16; o; o >>= 1) {
-        sscan += __shfl_xor_sync(0xffffffffu, sscan, o);
-        s32 += __shfl_xor_sync(0xffffffffu, s32, o);
-    }
-    if (lane == 0) {
-        atomicAdd(&s[0], npiv);
-        atomicAdd(&s[1], ein);
-        atomicAdd(&s[2], sdp);
-        atomicMax(&s[3], mdp);
-        atomicMax(&s[4], mid);
-        atomicAdd(&s[5], sscan);
-        atomicAdd(&s[6], sld);
-        atomicAdd(&s[7], sld2);
-        atomicAdd(&s[8], s32);
-    }
-    __syncthreads();
-    if (tid < kRawStats) out[(uint64_t)blockIdx.x * kRawStats + tid] = s[tid];
 }
 
 // Locates linear position q inside a list of position ranges.
@@ -149,11 +184,74 @@ bool variant_feasible(int v, const float* f) {
     }
 }
 
-static uint32_t chunk_of(int v) {
-    return (v == PC_VARIANT_BITMAP_WARP || v == PC_VARIANT_BITMAP_GROUP8 || v == PC_VARIANT_BITMAP_LANE)
-               ? (uint32_t)kChunkCta
-               : (uint32_t)kChunkWarp;
+static bool is_bitmap(int v) {
+    return v == PC_VARIANT_BITMAP_WARP || v == PC_VARIANT_BITMAP_GROUP8 || v == PC_VARIANT_BITMAP_LANE;
 }
+
+// Bitmap sets per CTA: K warps share one set; the smallest K whose 16/K sets
+// fit the shared-memory budget (about 100 KB for two CTAs per SM, up to
+// 200 KB for one).  Items carry 256*K in-neighbours.
+struct BitmapShape {
+    int K;
+    uint32_t words;
+    size_t smem;
+    int ctas_per_sm;
+    uint32_t chunk;
+};
+
+static BitmapShape bitmap_shape(uint32_t max_pivot_plus1) {
+    BitmapShape sh{};
+    sh.words = std::max<uint32_t>(1, (max_pivot_plus1 + 31) / 32);
+    const size_t budget_two = 100 * 1024, budget_one = 200 * 1024;
+    for (int K = 1; K <= 16; K *= 2) {
+        const size_t smem = (size_t)(16 / K) * sh.words * 4;
+        if (smem <= budget_two || (K == 16 && smem <= budget_one)) {
+            sh.K = K;
+            sh.smem = smem;
+            break;
+        }
+    }
+    if (!sh.K) {
+        sh.K = 16;
+        sh.smem = (size_t)sh.words * 4;
+    }
+    sh.ctas_per_sm = (int)std::max<size_t>(1, std::min<size_t>(4, (220 * 1024) / (sh.smem + 1024)));
+    sh.chunk = 256u * (uint32_t)sh.K;
+    return sh;
+}
+
+template <int K, int G>
+static pc_status launch_bitmap_kg(unsigned grid, size_t smem, cudaStream_t s, const uint64_t* off, const int32_t* adj,
+                                  const uint32_t* dp, const int32_t* plist, const Item* items, const uint32_t* nitems,
+                                  uint32_t* next, unsigned long long* total, uint32_t words, uint32_t chunk) {
+    PC_CUDA(cudaFuncSetAttribute(k_tc_bitmap<K, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_tc_bitmap<K, G><<<grid, kCtaThreads, smem, s>>>(off, adj, dp, plist, items, nitems, next, total, words, chunk);
+    return PC_OK;
+}
+
+template <int K>
+static pc_status launch_bitmap_k(int G, unsigned grid, size_t smem, cudaStream_t s, const uint64_t* off,
+                                 const int32_t* adj, const uint32_t* dp, const int32_t* plist, const Item* items,
+                                 const uint32_t* nitems, uint32_t* next, unsigned long long* total, uint32_t words,
+                                 uint32_t chunk) {
+    if (G == 32) return launch_bitmap_kg<K, 32>(grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
+    if (G == 8) return launch_bitmap_kg<K, 8>(grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
+    return launch_bitmap_kg<K, 1>(grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
+}
+
+static pc_status launch_bitmap(int K, int G, unsigned grid, size_t smem, cudaStream_t s, const uint64_t* off,
+                               const int32_t* adj, const uint32_t* dp, const int32_t* plist, const Item* items,
+                               const uint32_t* nitems, uint32_t* next, unsigned long long* total, uint32_t words,
+                               uint32_t chunk) {
+    switch (K) {
+        case 1: return launch_bitmap_k<1>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
+        case 2: return launch_bitmap_k<2>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
+        case 4: return launch_bitmap_k<4>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
+        case 8: return launch_bitmap_k<8>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
+        default: return launch_bitmap_k<16>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
+    }
+}
+
 
 }  // namespace tc
 
@@ -163,20 +261,29 @@ static pc_status tc_features(pc_pgraph* pg) {
     PC_TRY(ensure_dplus(pg));
     build_units(pg, &pg->unit_lo, &pg->unit_hi);
     const size_t U = pg->unit_lo.size();
+    const uint64_t n = pg->g->n;
     pg->part_features.assign(U * kNumFeatures, 0.f);
     if (U == 0) return PC_OK;
+    PC_TRY(pg->unit_of.ensure(std::max<uint64_t>(n, 1) * 4, "unit of vertex"));
     PC_TRY(scratch_reserve(pg, U * 16 + U * kRawStats * 8));
     int64_t* d_lo = nullptr;
     int64_t* d_hi = nullptr;
     PC_TRY(upload(pg, pg->unit_lo.data(), U, &d_lo));
     PC_TRY(upload(pg, pg->unit_hi.data(), U, &d_hi));
     unsigned long long* d_raw = pg->scratch.take<unsigned long long>(U * kRawStats);
+    cudaStream_t s = pg->g->stream;
+    PC_CUDA(cudaMemsetAsync(d_raw, 0, U * kRawStats * 8, s));
     const int32_t* plist = pg->contiguous ? nullptr : pg->new2old.as<int32_t>();
-    k_unit_stats<<<(unsigned)U, 256, 0, pg->g->stream>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), plist, d_lo,
-                                                        d_hi, d_raw);
+    int32_t* unit_of = pg->unit_of.as<int32_t>();
+    const int sms = sm_count(pg->g->device);
+    k_unit_of<<<(unsigned)U, 256, 0, s>>>(plist, d_lo, d_hi, unit_of);
+    PC_LAUNCHED();
+    k_unit_pivot_stats<<<sms * 8, 256, 0, s>>>(pg->off, pg->dplus.as<uint32_t>(), unit_of, n, d_raw);
+    PC_LAUNCHED();
+    k_unit_scan_stats<<<sms * 16, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), unit_of, n, d_raw);
     PC_LAUNCHED();
     std::vector<unsigned long long> raw(U * kRawStats);
-    PC_CUDA(cudaMemcpyAsync(raw.data(), d_raw, raw.size() * 8, cudaMemcpyDeviceToHost, pg->g->stream));
+    PC_CUDA(cudaMemcpyAsync(raw.data(), d_raw, raw.size() * 8, cudaMemcpyDeviceToHost, s));
     PC_TRY(sync(pg));
     for (size_t u = 0; u < U; ++u) raw_to_features(&raw[u * kRawStats], &pg->part_features[u * kNumFeatures]);
     return PC_OK;
@@ -205,7 +312,7 @@ static pc_status run_variant(pc_pgraph* pg, int v, const std::vector<int64_t>& r
     int64_t* d_pref = nullptr;
     PC_TRY(upload(pg, ranges.data(), ranges.size(), &d_ranges));
     PC_TRY(upload(pg, pref.data(), nr + 1, &d_pref));
-    const uint32_t chunk = chunk_of(v);
+    const uint32_t chunk = is_bitmap(v) ? bitmap_shape(max_pivot_plus1).chunk : (uint32_t)kChunkWarp;
     uint32_t* d_cnt = pg->scratch.take<uint32_t>(npos + 1);
     uint32_t* d_start = pg->scratch.take<uint32_t>(npos + 1);
     size_t tmpb = 0;
@@ -227,20 +334,12 @@ static pc_status run_variant(pc_pgraph* pg, int v, const std::vector<int64_t>& r
     *launches += 3;
     const uint32_t* d_nitems = d_start + npos;
     if (v == PC_VARIANT_BITMAP_WARP || v == PC_VARIANT_BITMAP_GROUP8 || v == PC_VARIANT_BITMAP_LANE) {
-        const uint32_t words = (max_pivot_plus1 + 31) / 32;
-        const size_t smem = (size_t)words * 4;
-        const int ctas_per_sm = smem <= 24 * 1024 ? 4 : (smem <= 48 * 1024 ? 2 : 1);
-        const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms * ctas_per_sm, item_bound));
-#define PC_LAUNCH_BM(G)                                                                                        \
-    do {                                                                                                       \
-        PC_CUDA(cudaFuncSetAttribute(k_tc_bitmap<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-        k_tc_bitmap<G><<<grid, kCtaThreads, smem, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems, d_next, \
-                                                       d_total, words);                                        \
-    } while (0)
-        if (v == PC_VARIANT_BITMAP_WARP) PC_LAUNCH_BM(32);
-        else if (v == PC_VARIANT_BITMAP_GROUP8) PC_LAUNCH_BM(8);
-        else PC_LAUNCH_BM(1);
-#undef PC_LAUNCH_BM
+        const BitmapShape sh = bitmap_shape(max_pivot_plus1);
+        const unsigned grid =
+            (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms * sh.ctas_per_sm, item_bound));
+        const int Gsel = v == PC_VARIANT_BITMAP_WARP ? 32 : (v == PC_VARIANT_BITMAP_GROUP8 ? 8 : 1);
+        PC_TRY(launch_bitmap(sh.K, Gsel, grid, sh.smem, s, pg->off, pg->adj, dp, plist, d_items, d_nitems, d_next,
+                             d_total, sh.words, chunk));
     } else {
         const unsigned grid = (unsigned)std::max<uint64_t>(
             1, std::min<uint64_t>((uint64_t)sms * 8, ceil_div(item_bound, kWarpCtaWarps)));
@@ -267,25 +366,36 @@ static pc_status tc_execute(pc_pgraph* pg, const std::vector<int8_t>& assign, ui
     const std::vector<int64_t>& hi = pg->unit_hi;
     const std::vector<float>& feat = pg->part_features;
     const size_t U = lo.size();
+    // One launch group per variant; bitmap variants are further split by the
+    // shape (warps per bitmap set) their units' id ranges need, so hub units
+    // keep warp-private bitmaps.
     struct Group {
+        int v = -1;
         std::vector<int64_t> ranges;
         uint64_t npos = 0, item_bound = 0;
         uint32_t maxid = 0;
-    } groups[PC_NUM_VARIANTS];
+    };
+    std::vector<Group> groups(PC_NUM_VARIANTS * 5);
     for (size_t u = 0; u < U; ++u) {
         const int v = assign[u];
         if (v < 0) continue;
-        Group& gr = groups[v];
+        const uint32_t mid = (uint32_t)feat[u * kNumFeatures + 4];
+        int key = v * 5;
+        if (is_bitmap(v)) {
+            const int K = bitmap_shape(mid).K;
+            key += K == 1 ? 0 : K == 2 ? 1 : K == 4 ? 2 : K == 8 ? 3 : 4;
+        }
+        Group& gr = groups[key];
+        gr.v = v;
         if (!gr.ranges.empty() && gr.ranges.back() == lo[u]) gr.ranges.back() = hi[u];
         else { gr.ranges.push_back(lo[u]); gr.ranges.push_back(hi[u]); }
         gr.npos += (uint64_t)(hi[u] - lo[u]);
-        // items <= pivots + in-edges / chunk
-        gr.item_bound += (uint64_t)(hi[u] - lo[u]) + (uint64_t)(feat[u * kNumFeatures + 1] / chunk_of(v)) + 1;
-        gr.maxid = std::max(gr.maxid, (uint32_t)feat[u * kNumFeatures + 4]);
+        // items <= pivots + in-edges / 256 (the smallest chunk)
+        gr.item_bound += (uint64_t)(hi[u] - lo[u]) + (uint64_t)(feat[u * kNumFeatures + 1] / 256.0) + 1;
+        gr.maxid = std::max(gr.maxid, mid);
     }
     size_t need = 1024;
-    for (int v = 0; v < PC_NUM_VARIANTS; ++v) {
-        const Group& gr = groups[v];
+    for (const Group& gr : groups) {
         if (gr.ranges.empty()) continue;
         size_t tmpb = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, tmpb, (uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t)(gr.npos + 1), s);
@@ -296,10 +406,9 @@ static pc_status tc_execute(pc_pgraph* pg, const std::vector<int8_t>& assign, ui
     uint64_t launches = 0;
     PC_CUDA(cudaEventRecord(pg->ev0, s));
     PC_CUDA(cudaMemsetAsync(d_total, 0, 8, s));
-    for (int v = 0; v < PC_NUM_VARIANTS; ++v) {
-        const Group& gr = groups[v];
+    for (const Group& gr : groups) {
         if (gr.ranges.empty()) continue;
-        PC_TRY(run_variant(pg, v, gr.ranges, gr.item_bound, gr.maxid, d_total, &launches));
+        PC_TRY(run_variant(pg, gr.v, gr.ranges, gr.item_bound, gr.maxid, d_total, &launches));
     }
     PC_CUDA(cudaEventRecord(pg->ev1, s));
     unsigned long long h = 0;

@@ -66,8 +66,44 @@ __device__ __forceinline__ uint32_t scan_prefix(const int32_t* __restrict__ row,
     return hits;
 }
 
-// CTA-wide bitmap kernel (persistent grid; one item at a time per CTA).
+// Named barrier over `nthreads` threads of one warp group (ids 1..15; id 0
+// is __syncthreads).
+__device__ __forceinline__ void group_barrier(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Pipelined group-of-G prefix scan: the load of the next G ids is issued
+// before the current ones are tested, so two loads per lane are in flight.
+// Stops at the first id >= b and never reads past lim = dplus[c].
 template <int G>
+__device__ __forceinline__ uint32_t scan_prefix_pipelined(const int32_t* __restrict__ row, uint32_t lim, int32_t b,
+                                                          int gl, unsigned gmask,
+                                                          const uint32_t* __restrict__ bm) {
+    uint32_t hits = 0;
+    uint32_t i = gl;
+    int32_t a = i < lim ? __ldg(row + i) : 0x7fffffff;
+    for (;;) {
+        const uint32_t inext = i + G;
+        const int32_t an = inext < lim ? __ldg(row + inext) : 0x7fffffff;
+        if (a < b) hits += (bm[a >> 5] >> (a & 31)) & 1u;
+        int32_t last;
+        if constexpr (G == 1) last = a;
+        else last = __shfl_sync(gmask, a, G - 1, G);
+        if (last >= b) break;
+        a = an;
+        i = inext;
+    }
+    return hits;
+}
+
+// Bitmap kernel: a CTA of kCtaThreads threads holds 16/K pivot bitmaps in
+// shared memory, one per group of K warps; each group takes its own work
+// items (pivot, <= 256*K in-neighbours), so a group synchronises only with
+// itself (a named barrier, or nothing when K == 1).  In-neighbour metadata
+// (id, row offset, prefix length) is fetched 32 at a time with one coalesced
+// load and 32 independent gathers, then handed to groups of G lanes by
+// shuffles; each group scans one prefix with scan_prefix_pipelined.
+template <int K, int G>
 __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __restrict__ off,
                                                            const int32_t* __restrict__ adj,
                                                            const uint32_t* __restrict__ dplus,
@@ -76,47 +112,65 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
                                                            const uint32_t* __restrict__ nitems_p,
                                                            uint32_t* __restrict__ next_item,
                                                            unsigned long long* __restrict__ total,
-                                                           uint32_t bm_words) {
-    extern __shared__ uint32_t bm[];
-    __shared__ uint32_t s_item;
-    __shared__ unsigned long long s_sum;
-    const int tid = threadIdx.x;
-    for (uint32_t i = tid; i < bm_words; i += blockDim.x) bm[i] = 0;
-    if (tid == 0) s_sum = 0;
+                                                           uint32_t bm_words, uint32_t chunk) {
+    extern __shared__ uint32_t smem[];
+    __shared__ uint32_t s_item[16];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int set = warp / K, wi = warp % K;
+    const int nsets = (kCtaThreads / 32) / K;
+    const int set_threads = K * 32, tis = wi * 32 + lane;
+    uint32_t* bm = smem + (size_t)set * bm_words;
+    for (uint32_t i = tid; i < (uint32_t)nsets * bm_words; i += blockDim.x) smem[i] = 0;
+    __syncthreads();
+    auto set_sync = [&]() {
+        if constexpr (K == 1) __syncwarp();
+        else group_barrier(1 + set, set_threads);
+    };
     const uint32_t nitems = *nitems_p;
-    const int lane = tid & 31;
-    const int group = tid / G, ngroups = blockDim.x / G, gl = tid % G;
+    constexpr int NG = 32 / G;  // in-neighbours handled at once per warp
+    const int gidx = lane / G, gl = lane % G;
     const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
     unsigned long long cnt = 0;
     for (;;) {
-        __syncthreads();
-        if (tid == 0) s_item = atomicAdd(next_item, 1u);
-        __syncthreads();
-        const uint32_t it = s_item;
+        if (tis == 0) s_item[set] = atomicAdd(next_item, 1u);
+        set_sync();
+        const uint32_t it = s_item[set];
         if (it >= nitems) break;
         const Item I = items[it];
         const int32_t b = pivot_at(plist, I.pos);
         const uint64_t rb = off[b], re = off[b + 1];
         const uint32_t dp = dplus[b];
-        for (uint32_t k = tid; k < dp; k += blockDim.x) {
+        for (uint32_t k = tis; k < dp; k += set_threads) {
             const int32_t a = adj[rb + k];
             atomicOr(&bm[a >> 5], 1u << (a & 31));
         }
-        __syncthreads();
+        set_sync();
         const uint64_t in0 = rb + dp + (uint64_t)I.j0;
-        const uint64_t in1 = min(in0 + (uint64_t)kChunkCta, re);
-        for (uint64_t e = in0 + group; e < in1; e += ngroups) {
-            const int32_t c = adj[e];
-            cnt += scan_prefix<G>(adj + off[c], dplus[c], b, gl, gmask,
-                                  [&](int32_t a) -> uint32_t { return (bm[a >> 5] >> (a & 31)) & 1u; });
+        const uint64_t in1 = min(in0 + (uint64_t)chunk, re);
+        for (uint64_t base = in0 + (uint64_t)wi * 32; base < in1; base += (uint64_t)set_threads) {
+            const uint64_t e = base + lane;
+            const bool ok = e < in1;
+            const int32_t c = ok ? adj[e] : 0;
+            const uint64_t rc = ok ? off[c] : 0;
+            const uint32_t lim = ok ? dplus[c] : 0;
+            const uint64_t left = in1 - base;
+            const int nb = left < 32 ? (int)left : 32;
+            for (int j0 = 0; j0 < 32; j0 += NG) {
+                if (j0 >= nb) break;
+                const int j = j0 + gidx;
+                const int src = j < nb ? j : 0;
+                const uint64_t rcj = __shfl_sync(0xffffffffu, rc, src);
+                uint32_t limj = __shfl_sync(0xffffffffu, lim, src);
+                if (j >= nb) limj = 0;
+                if (limj) cnt += scan_prefix_pipelined<G>(adj + rcj, limj, b, gl, gmask, bm);
+            }
         }
-        __syncthreads();
-        for (uint32_t k = tid; k < dp; k += blockDim.x) bm[adj[rb + k] >> 5] = 0;
+        set_sync();
+        for (uint32_t k = tis; k < dp; k += set_threads) bm[adj[rb + k] >> 5] = 0;
+        set_sync();
     }
     for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-    if (lane == 0 && cnt) atomicAdd(&s_sum, cnt);
-    __syncthreads();
-    if (tid == 0 && s_sum) atomicAdd(total, s_sum);
+    if (lane == 0 && cnt) atomicAdd(total, cnt);
 }
 
 __device__ __forceinline__ uint32_t hash_slot(int32_t a) { return ((uint32_t)a * 0x9E3779B1u) >> (32 - 9); }

@@ -278,3 +278,21 @@ def test_config1_rmat16(gpu, O):
     assert int(lab.astype(np.int64).sum()) == s["cdlp_sum"]
     lcc = pg.solve_lcc_merge()
     assert int(np.isnan(lcc).sum()) == s["lcc_nan"]
+
+
+def test_bitmap_kernels_every_set_shape(gpu, O):
+    """Forced bitmap variants on RMAT-20 with 64 partitions: pivot ids up to
+    2^20 make the kernels share one bitmap among K = 1, 2, 4, 8 and 16 warps
+    (named barriers) across the units; the count must not change."""
+    pc = gpu
+    h = pc.HostCSR.rmat(20, 16, 5)
+    vl, el, _ = h.arrays()
+    n = vl.size - 1
+    t = O.tc_merge(vl, el)
+    pg = pc.Partitioned_Graph(pc.Graph(vlist=vl, elist=el), pc.equal_vertex_partition(n, 64))
+    for name in ("bitmap_warp", "bitmap_group8", "bitmap_lane"):
+        assert pg.triangle_count(variant=pc.VARIANTS[name]) == t, name
+    assert pg.triangle_count(variant=pc.VARIANT_HEURISTIC) == t
+    f = pc.selector.unit_features(pg)
+    assert f[:, 1].sum() == el.size // 2  # every in-edge belongs to one unit
+    assert (f[:, 0].sum(), f[:, 4].max()) == (n, n)
