@@ -56,6 +56,14 @@ def parse():
     ap.add_argument("--cpu-sample-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--train-scale", type=int, default=22)
+    ap.add_argument("--batch", action="store_true",
+                    help="many-graph workload: 4096 RMAT graphs (scale 10..16, ef 8..32, seeds 0..4095), "
+                         "TC + LCC + BFS in one persistent launch")
+    ap.add_argument("--batch-graphs", type=int, default=4096)
+    ap.add_argument("--suite", default="",
+                    help="comma list of per-config suites: algos (RMAT-22, P=256, all nine algorithms with full-size "
+                         "parity against the reference on the host cores), skew (ER and Chung-Lu, n=2^24, m=2^28, "
+                         "P=512), rmat25 (RMAT-25, P=2048); one JSON line per measurement")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: plain heuristic plan only, no selector training, e2e or CPU leg")
     return ap.parse_args()
@@ -216,7 +224,8 @@ def reference_tc_sample(vl, el, target_s, threads):
             break
         k = max(1, int(k * max(dt, 1e-3) / target_s * 1.5)) if dt > 0.05 else max(1, k // 16)
     gteps = e_plus / (dt * k) / 1e9
-    sample = (f"rows u = 0 mod {k} ({rows.size} of {n} rows) of the RMAT-24 graph, "
+    sample = (f"the reference's TC loop (body and static OpenMP schedule of Graph::solve_triangle_counting_merge) "
+              f"over rows u = 0 mod {k} ({rows.size} of {n} rows) of the RMAT-{int(np.log2(n))} graph, "
               f"{dt:.2f} s, extrapolated x{k}")
     return gteps, kind, sample, R, run, rows, k, e_plus
 
@@ -270,12 +279,32 @@ def train_selector(pc, args):
         n = vl.size - 1
         g = pc.Graph(vlist=vl, elist=el)
         pg = pc.Partitioned_Graph(g, pc.equal_vertex_partition(n, max(1, n // 16384)))
-        sel.collect(pg, max_units=96, repeats=2)
+        sel.collect_insitu(pg, repeats=2)
         pg.close()
         g.close()
     tuned = sel.autotune()
     loss = sel.train(steps=1500, lr=3e-3, seed=7)
-    return {"samples": sel.num_samples(), "train_loss": loss, "heuristic_params": tuned.tolist()}
+    return {"samples": sel.num_samples(), "train_loss": loss, "heuristic_params": tuned.tolist(),
+            "collection": "in-situ: every variant run on all units at once, each unit charged its cycle share"}
+
+
+def plan_bounds(pc, pg):
+    """Per-unit costs of every variant on this graph (one profiled full run
+    each), and what the plain and learned plans and the best variant per unit
+    add up to under them."""
+    sel = pc.selector
+    n0 = sel.num_samples()
+    sel.collect_insitu(pg, repeats=1)
+    _, y, m = sel.samples()
+    y, m = y[n0:].astype(np.float64), m[n0:].astype(bool)
+    cost = np.where(m, np.exp(y), np.inf)
+    out = {"per_unit_best_ms": round(float(cost.min(axis=1).sum()), 3)}
+    for name, v in (("plain", pc.VARIANT_HEURISTIC), ("learned", pc.VARIANT_AUTO)):
+        plan = sel.plan(pg, v)
+        plan = plan[plan >= 0].astype(np.int64)
+        if plan.size == cost.shape[0]:
+            out[f"{name}_plan_ms"] = round(float(cost[np.arange(plan.size), plan].sum()), 3)
+    return out
 
 
 def time_device(pc, torch, pg, stream, variant, steps, warmup):
@@ -378,6 +407,7 @@ def run_ours(args, dist):
             e2e.append(dt)
     for a in pinned:
         L.lib.pc_host_unregister(L.ptr(a))
+    bounds = plan_bounds(pc, pg)
     e2e_s = dist.max(statistics.median(e2e))
     e2e_value = dist.world * e_plus / e2e_s / 1e9
     h2d = vl.nbytes + el.nbytes + v2p.nbytes
@@ -409,7 +439,8 @@ def run_ours(args, dist):
             },
             "learned_vs_plain": {"learned_ms": round(step_ms, 4), "plain_ms": round(plain_ms, 4),
                                  "speedup": round(plain_ms / step_ms, 4),
-                                 "plain_variants_per_unit": list(st_plain.variant_hist), **train},
+                                 "plain_variants_per_unit": list(st_plain.variant_hist),
+                                 "unit_cost_sums": bounds, **train},
             "e2e": {"value": round(e2e_value, 4), "unit": "GTEPS", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": 8, "ms_per_step": round(e2e_s * 1e3, 2)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
@@ -425,8 +456,262 @@ def run_ours(args, dist):
     g.close()
 
 
+def run_batch(args):
+    """Config 4: TC + LCC + BFS for every graph of the arena in one
+    persistent-kernel launch replayed from a captured CUDA graph, schedule
+    from the autotuner.  value = undirected edges of all graphs / launch time."""
+    import torch
+
+    import partitionandconquer_b200 as pc
+    from oracle import oracle as O
+    torch.cuda.set_device(0)
+    t0 = time.time()
+    h, voff = pc.HostCSR.rmat_batch(args.batch_graphs, 10, 16, 8, 32, seed=0)
+    vl, el, _ = h.arrays()
+    t_gen = time.time() - t0
+    G = voff.size - 1
+    b = pc.Batch(vl, el, voff)
+    tuned = b.autotune()
+    for _ in range(args.warmup):
+        r = b.run()
+    times = []
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            r = b.run()
+            times.append(r["ms"])
+    ms = statistics.median(times)
+    e_plus = el.size // 2
+    # verify a stratified sample of graphs against the oracle
+    rng = np.random.default_rng(0)
+    sample = sorted(set(rng.choice(G, size=min(G, 24), replace=False).tolist()))
+    cpu_s = 0.0
+    for g in sample:
+        v0, v1 = int(voff[g]), int(voff[g + 1])
+        sv = (vl[v0:v1 + 1] - vl[v0]).astype(np.uint64)
+        se = (el[vl[v0]:vl[v1]] - v0).astype(np.int32)
+        t = time.perf_counter()
+        tc = O.tc_merge(sv, se)
+        lcc = O.lcc(sv, se)
+        bfs = O.bfs(sv, se, 0)
+        cpu_s += time.perf_counter() - t
+        bad = [name for name, ok in (("tc", tc == int(r["tc"][g])), ("bfs", np.array_equal(bfs, r["bfs"][v0:v1])),
+                                     ("lcc", np.array_equal(lcc, r["lcc"][v0:v1], equal_nan=True))) if not ok]
+        if bad:
+            raise SystemExit(f"batch result mismatch on graph {g}: {bad}")
+    sample_edges = sum(int(vl[voff[g + 1]] - vl[voff[g]]) // 2 for g in sample)
+    line = {
+        "metric": "batched TC+LCC+BFS over 4096 RMAT graphs (undirected edges per second)", "value":
+            round(e_plus / (ms / 1e3) / 1e9, 4), "unit": "GTEPS", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded RMAT batch)",
+        "config": {"workload": f"batch{G}_rmat10-16_ef8-32", "graphs": G, "n": int(vl.size - 1),
+                   "m_directed": int(el.size), "tasks": "TC+LCC+BFS", "schedule": tuned,
+                   "launch": "one persistent kernel per step, replayed CUDA graph"},
+        "verified_graphs": len(sample),
+        "cpu_baseline": {"value": round(sample_edges / cpu_s / 1e9, 6), "unit": "GTEPS", "cores": os.cpu_count(),
+                         "kind": "port", "sample": f"oracle TC+LCC+BFS on {len(sample)} sampled graphs, {cpu_s:.1f} s"},
+        "clocks": clocks.summary(), "setup": {"graph_gen_s": round(t_gen, 1)},
+    }
+    print(json.dumps(line), flush=True)
+    b.close()
+
+
+# ---- per-config suites ------------------------------------------------------------
+
+def _timed(fn, steps, warmup):
+    """Median wall time of a synchronous library call (graph resident in HBM,
+    outputs copied to host inside the call) and its last result."""
+    out = None
+    for _ in range(warmup):
+        out = fn()
+    ts = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        out = fn()
+        ts.append(time.perf_counter() - t)
+    return statistics.median(ts), out
+
+
+def _cpu(fn):
+    t = time.perf_counter()
+    out = fn()
+    return time.perf_counter() - t, out
+
+
+def _rel_ok(a, b, tol):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    if a.shape != b.shape or not np.array_equal(np.isnan(a), np.isnan(b)):
+        return False, float("inf")
+    f = ~np.isnan(a)
+    den = np.maximum(np.abs(b[f]), 1e-300)
+    err = float(np.max(np.abs(a[f] - b[f]) / den)) if f.any() else 0.0
+    return err <= tol, err
+
+
+def _edge_sum_bytes(vl, el):
+    """SURVEY-style algorithmic bytes of the per-edge intersection sweep:
+    4 * sum over CSR entries (d(u) + d(v)) + 12 m + 8 (n + 1)."""
+    deg = np.diff(vl).astype(np.int64)
+    s = int((deg * deg).sum()) + int(deg[el].sum())
+    return 4 * s + 12 * el.size + 8 * deg.size + 8
+
+
+def suite_algos(pc, O, args, emit):
+    """Config 2: RMAT-22 ef16, 256 partitions, weights 1..255; every algorithm
+    on the GPU through the ABI against the reference's own OpenMP code (or the
+    oracle where the reference has no correct form of the computation) on the
+    host cores, outputs compared at full size."""
+    cores = os.cpu_count() or 1
+    h = pc.HostCSR.rmat(22, 16, args.seed)
+    h.add_weights(seed=args.seed, wmax=255)
+    vl, el, w = h.arrays()
+    n, m = vl.size - 1, el.size
+    g = pc.Graph(vlist=vl, elist=el, weights=w)
+    pg = pc.Partitioned_Graph(g, pc.equal_vertex_partition(n, 256))
+    R = O.Reference(vl, el, w, threads=cores) if O.Reference.available() else None
+    peak, peak_kind = hbm_peak()
+    lab0 = np.arange(n, dtype=np.int32)
+    prio = pc.vertex_priority(args.seed, n)
+    tc_bytes = tc_algorithmic_bytes(vl, el)[0]
+    es_bytes = _edge_sum_bytes(vl, el)
+    sweep = 4 * m + 8 * (n + 1) + 4 * n
+    cases = [
+        # name, gpu call, cpu (kind, call), units, bytes, compare
+        # the reference's own TC and LCC loops take minutes here (static OpenMP schedule over
+        # degree-sorted rows: 91 s for TC on 16 cores); the oracle (dynamic schedule) checks them
+        ("tc", lambda: pg.triangle_count(), ("port", lambda: O.tc_merge(vl, el)), m // 2, tc_bytes, "exact"),
+        ("tc_galloping", lambda: pg.solve_triangle_counting_galloping(), None, m // 2, tc_bytes, "exact6"),
+        ("lcc", lambda: pg.solve_lcc_merge(), ("port", lambda: O.lcc(vl, el)), m, es_bytes, 1e-6),
+        ("jaccard_edges", lambda: pg.jaccard_edges(), ("port", lambda: O.jaccard_edges(vl, el)), m, es_bytes, 1e-6),
+        ("bfs", lambda: pg.solve_bfs(0), ("port", lambda: O.bfs(vl, el, 0)), m, sweep, "exact"),
+        ("sssp", lambda: pg.solve_sssp(0), ("port", lambda: O.sssp(vl, el, w, 0)), m, sweep, "exact"),
+        ("pagerank_fp32", lambda: pg.page_rank(0.85, 20), ("port", lambda: O.pagerank_f64(vl, el, 0.85, 20)),
+         m * 20, 20 * (8 * m + 20 * n), 1e-6),
+        ("pagerank_fp64", lambda: pg.page_rank(0.85, 20, fp64=True),
+         ("port", lambda: O.pagerank_f64(vl, el, 0.85, 20)), m * 20, 20 * (12 * m + 24 * n), 1e-12),
+        ("kcore", lambda: pg.solve_kcore(), ("reference", lambda: R.kcore()) if R else ("port", lambda: O.kcore(vl, el)),
+         m, sweep, "exact"),
+        ("mis", lambda: pg.solve_mis(), ("reference", lambda: R.mis()) if R else ("port", lambda: O.mis(vl, el)),
+         m, sweep, "exact"),
+        ("mis_hashed", lambda: pg.solve_mis(seed=args.seed), ("port", lambda: O.mis(vl, el, priority=prio)),
+         m, sweep, "exact"),
+        ("cdlp", lambda: pg.solve_cdlp(lab0, 10),
+         ("reference", lambda: R.cdlp(lab0, 10)) if R else ("port", lambda: O.cdlp(vl, el, lab0, 10)),
+         m * 10, 10 * sweep, "exact"),
+    ]
+    ref_tc = None
+    for name, gpu, cpu, units, nbytes, cmp in cases:
+        t_gpu, out = _timed(gpu, args.steps, args.warmup)
+        rec = {"suite": "algos", "workload": "rmat22_ef16_p256_w255", "algorithm": name, "n": int(n),
+               "m_directed": int(m), "gpu_ms": round(t_gpu * 1e3, 3), "gteps": round(units / t_gpu / 1e9, 4),
+               "algorithmic_gbs": round(nbytes / t_gpu / 1e9, 1), "hbm_frac": round(nbytes / t_gpu / 1e9 / peak, 4),
+               "peak_kind": peak_kind}
+        if cpu is None:
+            ok, err = (int(out) == 6 * ref_tc), 0.0
+            rec.update({"parity": "exact (6 T)" if ok else "MISMATCH"})
+        else:
+            kind, fn = cpu
+            t_cpu, want = _cpu(fn)
+            if name == "tc":
+                ref_tc = int(want)
+            if cmp == "exact":
+                ok = int(out) == int(want) if np.isscalar(want) or isinstance(want, int) else \
+                    np.array_equal(np.asarray(out), np.asarray(want))
+                err = 0.0
+            else:
+                ok, err = _rel_ok(out, want, cmp)
+            rec.update({"cpu_ms": round(t_cpu * 1e3, 1), "cpu_kind": kind, "cpu_cores": cores,
+                        "speedup_vs_cpu": round(t_cpu / t_gpu, 1),
+                        "parity": ("exact" if cmp == "exact" else f"max rel err {err:.2e} <= {cmp}")
+                        if ok else f"MISMATCH (err {err})"})
+        emit(rec)
+    if R is not None:
+        R.close()
+    pg.close()
+    g.close()
+
+
+def _learned_vs_plain(pc, torch, pg, stream, steps, warmup):
+    tl, kl, cl, _, stl = time_device(pc, torch, pg, stream, pc.VARIANT_AUTO, steps, warmup)
+    tp, kp, cp, _, stp = time_device(pc, torch, pg, stream, pc.VARIANT_HEURISTIC, steps, warmup)
+    if len(cl | cp) != 1:
+        raise SystemExit(f"learned and plain counts differ: {cl | cp}")
+    return {"triangles": int(cl.pop()), "learned_ms": round(statistics.median(kl), 3),
+            "plain_ms": round(statistics.median(kp), 3),
+            "speedup": round(statistics.median(kp) / statistics.median(kl), 4),
+            "learned_variants": list(stl.variant_hist), "plain_variants": list(stp.variant_hist)}
+
+
+def suite_selector_graph(pc, O, torch, args, emit, name, h, P, suite):
+    vl, el, _ = h.arrays()
+    n, m = vl.size - 1, el.size
+    algo_bytes, W, e_plus = tc_algorithmic_bytes(vl, el)
+    g = pc.Graph(vlist=vl, elist=el)
+    pg = pc.Partitioned_Graph(g, pc.equal_vertex_partition(n, P))
+    stream = torch.cuda.ExternalStream(g.stream())
+    lp = _learned_vs_plain(pc, torch, pg, stream, args.steps, args.warmup)
+    lp["unit_cost_sums"] = plan_bounds(pc, pg)
+    peak, peak_kind = hbm_peak()
+    kms = lp["learned_ms"]
+    t_j, jac = _timed(lambda: pg.jaccard_edges(), max(1, args.steps // 2), 1)
+    # Jaccard spot check: the oracle's formula on a sample of rows
+    rows = np.arange(0, n, max(1, n // 500), dtype=np.int64)
+    bad = 0
+    deg = np.diff(vl).astype(np.int64)
+    for u in rows[:500]:
+        nu = el[vl[u]:vl[u + 1]]
+        for k, v in enumerate(nu[:16]):
+            c = np.intersect1d(nu, el[vl[v]:vl[v + 1]], assume_unique=True).size
+            want = np.float32(c / (deg[u] + deg[v] - c))
+            if jac[vl[u] + k] != want:
+                bad += 1
+    gteps_cpu, kind, sample, Rf, *_ = reference_tc_sample(vl, el, args.cpu_sample_seconds, os.cpu_count() or 1)
+    if Rf is not None:
+        Rf.close()
+    emit({"suite": suite, "workload": f"{name}_p{P}", "n": int(n), "m_directed": int(m), **lp,
+          "tc_gteps_learned": round(e_plus / (kms / 1e3) / 1e9, 4),
+          "tc_roofline_frac": round(algo_bytes / (kms / 1e3) / 1e9 / peak, 4), "peak_kind": peak_kind,
+          "W": int(W), "jaccard_ms": round(t_j * 1e3, 3), "jaccard_gteps": round(m / t_j / 1e9, 4),
+          "jaccard_spot_mismatches": bad,
+          "cpu_tc_gteps": gteps_cpu, "cpu_kind": kind, "cpu_cores": os.cpu_count(), "cpu_sample": sample})
+    pg.close()
+    g.close()
+
+
+def run_suites(args):
+    import torch
+
+    import partitionandconquer_b200 as pc
+    from oracle import oracle as O
+    torch.cuda.set_device(0)
+
+    def emit(rec):
+        print(json.dumps(rec), flush=True)
+
+    names = [x for x in args.suite.split(",") if x]
+    if "algos" in names:
+        suite_algos(pc, O, args, emit)
+    if "skew" in names or "rmat25" in names:
+        emit({"suite": "selector", "training": train_selector(pc, args)})
+    if "skew" in names:
+        suite_selector_graph(pc, O, torch, args, emit, "er24_m2^28",
+                             pc.HostCSR.er(24, 1 << 28, args.seed), 512, "skew")
+        suite_selector_graph(pc, O, torch, args, emit, "chunglu24_m2^28_b2.1_dmax2^20",
+                             pc.HostCSR.chung_lu(24, 1 << 28, 2.1, 1 << 20, args.seed), 512, "skew")
+    if "rmat25" in names:
+        suite_selector_graph(pc, O, torch, args, emit, "rmat25_ef16",
+                             pc.HostCSR.rmat(25, 16, args.seed), 2048, "rmat25")
+
+
 def main():
     args = parse()
+    if args.suite:
+        run_suites(args)
+        return
+    if args.batch:
+        run_batch(args)
+        return
     if args.impl == "reference":
         # the reference is a host-CPU program: rank 0 alone runs it, no process group
         if int(os.environ.get("RANK", "0")) == 0:

@@ -81,6 +81,36 @@ pc_status pc_graph_info(const pc_graph* g, uint64_t* n, uint64_t* m, int32_t* we
 /* Opaque cudaStream_t of the handle (for event timing by the caller). */
 void* pc_graph_stream(const pc_graph* g);
 
+/* ---- ingest on the device ------------------------------------------------ */
+
+#define PC_INGEST_DEGREE_RELABEL 1u /* relabel by descending degree, ties by id */
+
+/* Build a graph on the device from a raw edge stream (host arrays, nedges
+ * pairs, ids in [0, n)): both directions of every edge, self-loops dropped,
+ * rows sorted and deduplicated -- the adjacency build of the text loader
+ * Graph::Graph(file) (src/Graph.cpp:59-85, after parsing and without its id
+ * shift) and of the preprocess tool (src/preprocess.cpp:5-45).  With
+ * PC_INGEST_DEGREE_RELABEL the ids are relabelled by descending degree (ties
+ * by ascending id) and old2new (n entries, may be NULL) receives the map.
+ * Radix sort + unique + one pass on the device; the result equals the host
+ * builder's arrays bit for bit. */
+pc_status pc_graph_from_edges(const uint32_t* src, const uint32_t* dst, uint64_t nedges, uint64_t n, uint32_t flags,
+                              int32_t* old2new, pc_graph** out);
+/* Seeded synthetic graphs generated and built on the device; identical to
+ * pc_synth_rmat / pc_synth_er below (same counter-based edge streams). */
+pc_status pc_graph_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, uint32_t flags, pc_graph** out);
+pc_status pc_graph_er(uint32_t scale, uint64_t nedges, uint64_t seed, uint32_t flags, pc_graph** out);
+/* Symmetric integer weights in [1, wmax] keyed on the unordered endpoint
+ * pair, computed on the device (= pc_synth_add_weights).  The preprocess
+ * tool's weight file (src/preprocess.cpp:14-24) is the host path
+ * (pc::Graph::add_reference_weights).  Fails while a partitioned view of g
+ * exists. */
+pc_status pc_graph_add_weights(pc_graph* g, uint64_t seed, int32_t wmax);
+/* Copy the device CSR to host arrays (n+1 offsets, m ids, m weights; any may
+ * be NULL): the contents of csr_vlist.bin / csr_elist.bin / csr_weight.bin
+ * (Graph::save_as_csr_binfile, src/Graph.cpp:296-307). */
+pc_status pc_graph_download(const pc_graph* g, uint64_t* vlist, int32_t* elist, int32_t* weights);
+
 /* ---- partitioned graph (class Partitioned_Graph, src/Graph.hpp:105-155) -- */
 
 /* Build the partitioned view.  Replaces Partitioned_Graph::Partitioned_Graph
@@ -103,6 +133,15 @@ pc_status pc_pgraph_vertex_map(const pc_pgraph* pg, int32_t* old2new /* n */);
  * follow elist when the graph is weighted (may be NULL).  vlist has P*n+1
  * entries, elist/weights m.  Meant for small graphs and parity tests. */
 pc_status pc_pgraph_layout(pc_pgraph* pg, uint64_t* vlist, int32_t* elist, int32_t* weights);
+/* Graph::greedy_partition (src/Graph.cpp:898-967) on the GPU, seeded: the
+ * vertices with degree >= P, in descending-degree order, spread their
+ * unplaced neighbours over the partitions by the reference's quotas
+ * max(0, deg/P - placed_i); all other vertices get a seeded random
+ * partition (the reference's rule gives them zero quotas).  Heavy vertices
+ * run in waves of 64; a vertex does not see what the others of its wave
+ * place, the only difference from the sequential rule.  P <= 16384.
+ * v2p receives n partition ids. */
+pc_status pc_greedy_partition(pc_graph* g, int32_t P, uint64_t seed, int32_t* v2p);
 /* evaluate_partition (src/Graph.cpp:1460-1473): max part degree, max degree. */
 pc_status pc_pgraph_evaluate(pc_pgraph* pg, int64_t* max_part_deg, int64_t* max_deg, double* balance_ratio);
 
@@ -158,6 +197,18 @@ pc_status pc_batch_count_pairs(pc_pgraph* pg, const int32_t* pairs /* 2*nq */, u
  * set i is ids[offsets[i] .. offsets[i+1]) (at least 2 vertices). */
 pc_status pc_batch_count_sets(pc_pgraph* pg, const int32_t* ids, const uint64_t* offsets, uint64_t nq, uint64_t* out);
 
+/* Friend triangles around root (Partitioned_Graph::solve_friend_triangle_merge
+ * and _galloping, src/Graph.cpp:1222-1264; Graph:: forms src/Graph.cpp:309-340):
+ * the sum over positions j < k of nodes, both not the root, of
+ * |N(root) & N(nodes[j]) & N(nodes[k])|.  Both reference methods give this
+ * number.  Computed without enumerating the pairs: for every w in N(root),
+ * c_w positions are adjacent to it, and the sum is that of c_w (c_w - 1) / 2. */
+pc_status pc_friend_triangle(pc_pgraph* pg, int32_t root, const int32_t* nodes, uint64_t nn, uint64_t* out);
+/* Partitioned_Graph::solve_square_counting (src/Graph.cpp:1291-1324): the
+ * sum over u and v, w in N(u) with w < v < u of |N(v) & N(w) & [0, w)|, in
+ * the caller's vertex ids (after pc_pgraph_reorder, the reordered ones). */
+pc_status pc_square_count(pc_pgraph* pg, uint64_t* out);
+
 /* ---- frontier algorithms ----------------------------------------------- */
 
 /* Partitioned_Graph::solve_bfs (src/Graph.cpp:1701-1762) output convention:
@@ -208,6 +259,36 @@ pc_status pc_cdlp(pc_pgraph* pg, int32_t iterations, int32_t* labels);
 pc_status pc_tc_count_noalloc(const uint64_t* d_vlist, const int32_t* d_elist, uint64_t n, uint64_t m,
                               void* stream, uint64_t* count);
 
+/* ---- many graphs in one launch ---------------------------------------------
+ * No counterpart in the reference (which runs one graph per call).  G
+ * independent graphs packed in one CSR arena with arena-wide vertex ids:
+ * graph g owns vertices [voff[g], voff[g+1]) and no edge joins two graphs.
+ * pc_batch_run computes, for every graph, the tasks requested in one
+ * persistent-kernel launch replayed from a captured CUDA graph:
+ *   PC_BATCH_TC  tc[g]   triangles of graph g (solve_triangle_counting_merge);
+ *   PC_BATCH_LCC lcc[v]  Graph::solve_lcc_merge per arena vertex;
+ *   PC_BATCH_BFS bfs[v]  BFS level from graph g's first vertex, in
+ *                        Partitioned_Graph::solve_bfs's convention. */
+typedef struct pc_batch pc_batch;
+#define PC_BATCH_TC 1u
+#define PC_BATCH_LCC 2u
+#define PC_BATCH_BFS 4u
+typedef struct {
+    double ms;           /* device time of the replayed launch (CUDA events) */
+    uint32_t items;      /* (graph, task) work items */
+    int32_t threads;     /* threads per CTA */
+    int32_t ctas_per_sm; /* persistent CTAs per SM */
+    int32_t order;       /* 0 largest graphs first, 1 graph order */
+} pc_batch_stats;
+pc_status pc_batch_create(const uint64_t* vlist, const int32_t* elist, uint64_t N, uint64_t M, const uint64_t* voff,
+                          uint32_t G, pc_batch** out);
+pc_status pc_batch_destroy(pc_batch* b);
+pc_status pc_batch_run(pc_batch* b, uint32_t tasks, uint64_t* tc, double* lcc, int32_t* bfs, pc_batch_stats* stats);
+/* Schedule: threads 256|512, ctas_per_sm 1..4, order 0|1. */
+pc_status pc_batch_set_schedule(pc_batch* b, int32_t threads, int32_t ctas_per_sm, int32_t order);
+/* Times every schedule candidate on this batch and keeps the fastest. */
+pc_status pc_batch_autotune(pc_batch* b, uint32_t tasks, pc_batch_stats* best);
+
 /* ---- per-partition kernel selection (no counterpart in the reference: the
  *      reference runs one scalar merge everywhere) ------------------------- */
 
@@ -229,6 +310,12 @@ pc_status pc_tc_time_unit(pc_pgraph* pg, int32_t unit, int32_t variant, double* 
  * (heaviest first, then a stride over the rest), best of `repeats`; checks
  * that all variants return the same count. */
 pc_status pc_selector_collect(pc_pgraph* pg, int32_t max_units, int32_t repeats, int32_t* samples_added);
+/* Training data measured inside full runs: each variant runs on every unit it
+ * can take in one profiled call (best of `repeats`); the kernels charge their
+ * per-item warp-cycles to the units, and each unit's cost is its share of the
+ * measured launch time.  One sample per unit with work; counts are checked
+ * across the variants that ran on the same units. */
+pc_status pc_selector_collect_insitu(pc_pgraph* pg, int32_t repeats, int32_t* samples_added);
 int32_t pc_selector_num_samples(void);
 pc_status pc_selector_get_samples(float* feats, float* log_ms, uint8_t* mask, int32_t cap);
 pc_status pc_selector_add_samples(const float* feats, const float* log_ms, const uint8_t* mask, int32_t count);
@@ -281,6 +368,16 @@ pc_status pc_host_csr_save(const pc_host_csr* g, const char* dir);
 pc_status pc_host_csr_from_arrays(const uint64_t* vlist, const int32_t* elist, const int32_t* weights,
                                   uint64_t n, uint64_t m, pc_host_csr** out);
 pc_status pc_host_csr_free(pc_host_csr* g);
+/* G seeded RMAT graphs in one arena: graph g has scale in [smin, smax] and
+ * edge factor in [emin, emax] drawn from (seed, g), RMAT seed g, and is
+ * symmetrised, deduplicated and degree-relabelled; voff (G+1) receives the
+ * arena offsets of the graphs. */
+pc_status pc_synth_rmat_batch(uint32_t G, uint32_t smin, uint32_t smax, uint32_t emin, uint32_t emax, uint64_t seed,
+                              pc_host_csr** out, uint64_t* voff);
+/* The sequential seeded greedy partitioner on the host (src/Graph.cpp:898-967
+ * with one std::mt19937 in place of random_device and rand()). */
+pc_status pc_host_greedy_partition(const uint64_t* vlist, const int32_t* elist, uint64_t n, int32_t P, uint64_t seed,
+                                   int32_t* v2p);
 /* The priorities pc_mis_hashed orders vertices by: out[v] for v < n. */
 pc_status pc_synth_vertex_priority(uint64_t seed, uint64_t n, uint64_t* out);
 

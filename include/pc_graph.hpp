@@ -34,6 +34,10 @@ class Graph {
     // dropped, symmetrised, sorted, de-duplicated; ids shifted down by one
     // unless a 0 id appears (src/Graph.cpp:27-90).
     explicit Graph(const std::string graphfile);
+    // The same text loader with the adjacency build (symmetrise, sort,
+    // deduplicate) done on the GPU by pc_graph_from_edges; identical arrays.
+    struct OnDevice {};
+    Graph(const std::string graphfile, OnDevice);
     // Binary CSR directory: csr_vlist.bin / csr_elist.bin / csr_weight.bin
     // (src/Graph.cpp:92-137).  Throws on a missing or malformed file.
     Graph(const std::string csrdir, bool is_weighted);
@@ -71,6 +75,9 @@ class Graph {
     // algorithms on the GPU (unpartitioned forms; num_threads is accepted and ignored)
     size_t solve_triangle_counting_galloping(const int num_threads) const;
     size_t solve_triangle_counting_merge(const int num_threads) const;
+    // src/Graph.cpp:309-340
+    size_t solve_friend_triangle_galloping(const VID root, const std::vector<VID>& nodes, const int num_threads) const;
+    size_t solve_friend_triangle_merge(const VID root, const std::vector<VID>& nodes, const int num_threads) const;
     void batch_cnt_common_neis_merge(const std::vector<std::pair<VID, VID>>& queries, std::vector<size_t>& res,
                                      int num_threads) const;
     void batch_cnt_common_neis_merge(const std::vector<std::vector<VID>>& queries, std::vector<size_t>& res,
@@ -122,6 +129,10 @@ class Partitioned_Graph {
 
     size_t solve_triangle_counting_galloping() const;
     size_t solve_triangle_counting_merge() const;
+    // src/Graph.cpp:1222-1264 and 1291-1324
+    size_t solve_friend_triangle_galloping(const VID root, const std::vector<VID>& nodes) const;
+    size_t solve_friend_triangle_merge(const VID root, const std::vector<VID>& nodes) const;
+    size_t solve_square_counting() const;
     void batch_cnt_common_neis_merge(const std::vector<std::pair<VID, VID>>& queries, std::vector<size_t>& res) const;
     void batch_cnt_common_neis_merge(const std::vector<std::vector<VID>>& queries, std::vector<size_t>& res) const;
     void batch_cnt_common_neis_galloping(const std::vector<std::pair<VID, VID>>& queries,

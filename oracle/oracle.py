@@ -79,6 +79,8 @@ def _load_c():
         "or_mis": (None, [u64, P, P, P]),
         "or_mis_priority": (None, [u64, P, P, P, P]),
         "or_cdlp": (None, [u64, P, P, i32, P]),
+        "or_friend_triangle": (u64, [u64, P, P, i32, P, u64]),
+        "or_square_count": (u64, [u64, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -108,6 +110,17 @@ def _csr(vl, el):
 def tc_merge(vl, el):
     vl, el, n = _csr(vl, el)
     return int(clib().or_tc_merge(n, _ptr(vl), _ptr(el)))
+
+
+def friend_triangle(vl, el, root, nodes):
+    vl, el, n = _csr(vl, el)
+    q = np.ascontiguousarray(nodes, np.int32)
+    return int(clib().or_friend_triangle(n, _ptr(vl), _ptr(el), int(root), _ptr(q), q.size))
+
+
+def square_count(vl, el):
+    vl, el, n = _csr(vl, el)
+    return int(clib().or_square_count(n, _ptr(vl), _ptr(el)))
 
 
 def tc_rows(vl, el, rows):
@@ -281,6 +294,8 @@ class Reference:
                 "ref_kcore": (None, [P, C.c_int, u64, C.c_int, P]),
                 "ref_mis": (None, [P, C.c_int, u64, C.c_int, P]),
                 "ref_cdlp": (None, [P, C.c_int, u64, C.c_int, C.c_int, P]),
+                "ref_friend_triangle": (u64, [P, C.c_int, C.c_int, i32, P, u64, C.c_int]),
+                "ref_square_count": (u64, [P]),
             }
             for name, (res, args) in sig.items():
                 fn = getattr(lib, name)
@@ -424,6 +439,16 @@ class Reference:
         out = np.empty(self.n, np.int32)
         self.lib().ref_mis(self._obj(partitioned), int(partitioned), self.n, self.threads, _ptr(out))
         return out
+
+    @_muted
+    def friend_triangle(self, root, nodes, partitioned=False, galloping=False):
+        q = np.ascontiguousarray(nodes, np.int32)
+        return int(self.lib().ref_friend_triangle(self._obj(partitioned), int(partitioned), int(galloping), root,
+                                                  _ptr(q), q.size, self.threads))
+
+    @_muted
+    def square_count(self):
+        return int(self.lib().ref_square_count(self._obj(True)))
 
     @_muted
     def cdlp(self, labels, iters=10, partitioned=False):

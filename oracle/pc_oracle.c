@@ -38,6 +38,60 @@ static uint64_t merge_cnt(const uint64_t* vl, const int32_t* el, int64_t u, int6
     return res;
 }
 
+/* |N(a) & N(b) & N(c)| by two sorted merges (the k-way
+ * Graph::cnt_common_neis_merge(q), src/Graph.cpp:255-307, for k = 3). */
+static uint64_t merge3(const uint64_t* vl, const int32_t* el, int32_t a, int32_t b, int32_t c) {
+    uint64_t i = vl[a], ie = vl[a + 1], j = vl[b], je = vl[b + 1], k = vl[c], ke = vl[c + 1], res = 0;
+    while (i < ie && j < je) {
+        if (el[i] < el[j]) { i++; continue; }
+        if (el[i] > el[j]) { j++; continue; }
+        int32_t x = el[i];
+        while (k < ke && el[k] < x) k++;
+        if (k < ke && el[k] == x) res++;
+        i++;
+        j++;
+    }
+    return res;
+}
+
+/* Graph::solve_friend_triangle_merge (src/Graph.cpp:326-340) and the
+ * partitioned forms (src/Graph.cpp:1222-1264, whose per-partition counts sum
+ * to the whole-list count): positions j < k of nodes, the root skipped. */
+uint64_t or_friend_triangle(uint64_t n, const uint64_t* vl, const int32_t* el, int32_t root, const int32_t* nodes,
+                            uint64_t nn) {
+    (void)n;
+    uint64_t res = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : res)
+    for (int64_t j = 0; j < (int64_t)nn; j++) {
+        if (nodes[j] == root) continue;
+        for (uint64_t k = (uint64_t)j + 1; k < nn; k++) {
+            if (nodes[k] == root) continue;
+            res += merge3(vl, el, root, nodes[j], nodes[k]);
+        }
+    }
+    return res;
+}
+
+/* Partitioned_Graph::solve_square_counting (src/Graph.cpp:1291-1324): for
+ * every u and v, w in N(u) with w < v < u, |N(v) & N(w) & [0, w)| (the
+ * reference sums the partition-local counts, which add up to this). */
+uint64_t or_square_count(uint64_t n, const uint64_t* vl, const int32_t* el) {
+    uint64_t res = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : res)
+    for (int64_t u = 0; u < (int64_t)n; u++) {
+        for (uint64_t i = vl[u]; i < vl[u + 1]; i++) {
+            int32_t v = el[i];
+            if (v >= u) break;
+            for (uint64_t j = vl[u]; j < vl[u + 1]; j++) {
+                int32_t w = el[j];
+                if (w >= v) break;
+                res += lt_merge(vl, el, v, w, w);
+            }
+        }
+    }
+    return res;
+}
+
 /* Graph::solve_triangle_counting_merge (src/Graph.cpp:355-368). */
 uint64_t or_tc_merge(uint64_t n, const uint64_t* vl, const int32_t* el) {
     uint64_t res = 0;

@@ -8,6 +8,9 @@ extern "C" {
 #endif
 
 uint64_t or_tc_merge(uint64_t n, const uint64_t* vl, const int32_t* el);
+uint64_t or_friend_triangle(uint64_t n, const uint64_t* vl, const int32_t* el, int32_t root, const int32_t* nodes,
+                            uint64_t nn);
+uint64_t or_square_count(uint64_t n, const uint64_t* vl, const int32_t* el);
 uint64_t or_tc_galloping(uint64_t n, const uint64_t* vl, const int32_t* el);
 uint64_t or_tc_rows(uint64_t n, const uint64_t* vl, const int32_t* el, const int32_t* rows, uint64_t nrows);
 int or_layout(uint64_t n, const uint64_t* vl, const int32_t* el, const int32_t* w, const int32_t* v2p, int32_t P,

@@ -83,7 +83,9 @@ uint64_t ref_tc_rows(void* g, const int32_t* rows, uint64_t nrows, int threads) 
     const EID* vl = G->get_csr_vlist();
     const VID* el = G->get_csr_elist();
     size_t res = 0;
-#pragma omp parallel for num_threads(threads) schedule(dynamic, 16) reduction(+ : res)
+    // the reference loop's own schedule: `omp parallel for` without a
+    // schedule clause (static) over the rows, as Graph::solve_triangle_counting_merge
+#pragma omp parallel for num_threads(threads) schedule(static) reduction(+ : res)
     for (int64_t i = 0; i < (int64_t)nrows; ++i) {
         VID u = rows[i];
         for (EID j = vl[u]; j < vl[u + 1]; ++j) {
@@ -199,5 +201,22 @@ void ref_cdlp(void* obj, int partitioned, uint64_t n, int iters, int threads, in
     else static_cast<Graph*>(obj)->solve_cdlp(l, iters, threads);
     std::memcpy(labels, l.data(), n * sizeof(int32_t));
 }
+
+// Friend triangles: Graph::solve_friend_triangle_{merge,galloping}
+// (src/Graph.cpp:309-340), Partitioned_Graph:: forms (src/Graph.cpp:1222-1264).
+uint64_t ref_friend_triangle(void* obj, int partitioned, int galloping, int32_t root, const int32_t* nodes,
+                             uint64_t nn, int threads) {
+    std::vector<VID> q(nodes, nodes + nn);
+    if (partitioned) {
+        auto* p = static_cast<Partitioned_Graph*>(obj);
+        return galloping ? p->solve_friend_triangle_galloping(root, q) : p->solve_friend_triangle_merge(root, q);
+    }
+    auto* g = static_cast<Graph*>(obj);
+    return galloping ? g->solve_friend_triangle_galloping(root, q, threads)
+                     : g->solve_friend_triangle_merge(root, q, threads);
+}
+
+// Partitioned_Graph::solve_square_counting (src/Graph.cpp:1291-1324).
+uint64_t ref_square_count(void* pg) { return static_cast<Partitioned_Graph*>(pg)->solve_square_counting(); }
 
 }  // extern "C"

@@ -21,10 +21,11 @@ from ._lib import (METHOD_GALLOPING, METHOD_MERGE, NUM_VARIANTS, VARIANT_AUTO, V
 
 __all__ = [
     "Graph", "Partitioned_Graph", "HostCSR", "PCError", "TCStats", "VARIANTS", "VARIANT_AUTO",
-    "VARIANT_HEURISTIC", "equal_vertex_partition", "device_count", "launch_count", "selector",
+    "VARIANT_HEURISTIC", "equal_vertex_partition", "device_count", "launch_count", "selector", "Batch",
 ]
 
 INT_MAX = 2**31 - 1
+INGEST_DEGREE_RELABEL = 1  # PC_INGEST_DEGREE_RELABEL
 
 
 def device_count() -> int:
@@ -91,6 +92,14 @@ class HostCSR:
         w = None if weights is None else _lib.as_array(weights, np.int32)
         return cls._make(lib.pc_host_csr_from_arrays, ptr(vl), ptr(el), ptr(w), vl.size - 1, el.size)
 
+    @classmethod
+    def rmat_batch(cls, G: int, smin: int = 10, smax: int = 16, emin: int = 8, emax: int = 32, seed: int = 0):
+        """G seeded RMAT graphs in one arena; returns (HostCSR, voff[G+1])."""
+        out = C.c_void_p()
+        voff = np.zeros(G + 1, np.uint64)
+        check(lib.pc_synth_rmat_batch(G, smin, smax, emin, emax, seed, C.byref(out), ptr(voff)))
+        return cls(out), voff
+
     def add_weights(self, seed: int = 1, wmax: int = 255) -> "HostCSR":
         check(lib.pc_synth_add_weights(self._h, seed, wmax))
         return self
@@ -149,6 +158,59 @@ class Graph:
         self._g = None
         self._pg = None
 
+    # -- built on the device (pc_graph_from_edges / pc_graph_rmat / pc_graph_er) --
+    @classmethod
+    def _adopt(cls, handle) -> "Graph":
+        """Wraps a device-built handle; the host arrays are downloaded once."""
+        n, m, w = C.c_uint64(), C.c_uint64(), C.c_int32()
+        check(lib.pc_graph_info(handle, C.byref(n), C.byref(m), C.byref(w)))
+        vl = np.empty(n.value + 1, np.uint64)
+        el = np.empty(m.value, np.int32)
+        wt = np.empty(m.value, np.int32) if w.value else None
+        check(lib.pc_graph_download(handle, ptr(vl), ptr(el), ptr(wt)))
+        obj = cls.__new__(cls)
+        obj.vlist, obj.elist, obj.weights = vl, el, wt
+        obj.validate = False
+        obj._g = handle
+        obj._pg = None
+        return obj
+
+    @classmethod
+    def from_edges(cls, src, dst, n: int, relabel: bool = True, return_map: bool = False):
+        """Symmetric, deduplicated CSR built on the GPU from a raw edge stream
+        (the text loader's adjacency build, src/Graph.cpp:59-85)."""
+        s = _lib.as_array(src, np.uint32)
+        d = _lib.as_array(dst, np.uint32)
+        if s.size != d.size:
+            raise ValueError("src and dst must have the same length")
+        o2n = np.empty(n, np.int32) if (relabel and return_map) else None
+        out = C.c_void_p()
+        check(lib.pc_graph_from_edges(ptr(s), ptr(d), s.size, n, INGEST_DEGREE_RELABEL if relabel else 0, ptr(o2n),
+                                      C.byref(out)))
+        g = cls._adopt(out)
+        return (g, o2n) if return_map else g
+
+    @classmethod
+    def rmat_device(cls, scale: int, edge_factor: int = 16, seed: int = 1, relabel: bool = True, wmax: int = 0,
+                    weight_seed: int = 1) -> "Graph":
+        """HostCSR.rmat's graph, generated and built on the GPU."""
+        out = C.c_void_p()
+        check(lib.pc_graph_rmat(scale, edge_factor, seed, INGEST_DEGREE_RELABEL if relabel else 0, C.byref(out)))
+        if wmax:
+            try:
+                check(lib.pc_graph_add_weights(out, weight_seed, wmax))
+            except Exception:
+                lib.pc_graph_destroy(out)
+                raise
+        return cls._adopt(out)
+
+    @classmethod
+    def er_device(cls, scale: int, nedges: int, seed: int = 1, relabel: bool = True) -> "Graph":
+        """HostCSR.er's graph, generated and built on the GPU."""
+        out = C.c_void_p()
+        check(lib.pc_graph_er(scale, nedges, seed, INGEST_DEGREE_RELABEL if relabel else 0, C.byref(out)))
+        return cls._adopt(out)
+
     # -- accessors (src/Graph.cpp:151-307) --
     def get_vertex_num(self) -> int:
         return int(self.vlist.size - 1)
@@ -196,6 +258,17 @@ class Graph:
         """Seeded stand-in for Graph::random_partition (src/Graph.cpp:564-570, which uses rand())."""
         rng = np.random.default_rng(seed)
         return rng.integers(0, partition_num, self.get_vertex_num(), dtype=np.int32)
+
+    def greedy_partition(self, partition_num: int, seed: int = 1, on_device: bool = True) -> np.ndarray:
+        """Graph::greedy_partition (src/Graph.cpp:898-967), seeded.  on_device:
+        the GPU form (pc_greedy_partition); otherwise the sequential host rule."""
+        out = np.empty(self.get_vertex_num(), np.int32)
+        if on_device:
+            check(lib.pc_greedy_partition(self._device(), partition_num, seed, ptr(out)))
+        else:
+            check(lib.pc_host_greedy_partition(ptr(self.vlist), ptr(self.elist), self.get_vertex_num(), partition_num,
+                                               seed, ptr(out)))
+        return out
 
     # -- device handles --
     def _device(self):
@@ -251,6 +324,11 @@ class Graph:
         return self._one_partition().batch_cnt_common_neis_merge(queries)
 
     batch_cnt_common_neis_galloping = batch_cnt_common_neis_merge
+
+    def solve_friend_triangle_merge(self, root: int, nodes, num_threads: int = 0) -> int:
+        return self._one_partition().solve_friend_triangle_merge(root, nodes)
+
+    solve_friend_triangle_galloping = solve_friend_triangle_merge
 
     def solve_bfs(self, u: int):
         """BFS levels from u (rank[u] = -1, unreached INT_MAX) -- the partitioned output convention."""
@@ -400,6 +478,22 @@ class Partitioned_Graph:
 
     batch_cnt_common_neis_galloping = batch_cnt_common_neis_merge
     batch_cnt_common_neis_merge_fine_grained = batch_cnt_common_neis_merge
+
+    def solve_friend_triangle_merge(self, root: int, nodes) -> int:
+        """Sum over node pairs (positions j < k, the root skipped) of
+        |N(root) & N(nodes[j]) & N(nodes[k])| (src/Graph.cpp:1222-1264)."""
+        q = _lib.as_array(nodes, np.int32)
+        out = C.c_uint64()
+        check(lib.pc_friend_triangle(self._pg, int(root), ptr(q), q.size, C.byref(out)))
+        return int(out.value)
+
+    solve_friend_triangle_galloping = solve_friend_triangle_merge
+
+    def solve_square_counting(self) -> int:
+        """Partitioned_Graph::solve_square_counting (src/Graph.cpp:1291-1324)."""
+        out = C.c_uint64()
+        check(lib.pc_square_count(self._pg, C.byref(out)))
+        return int(out.value)
     batch_cnt_common_neis_galloping_fine_grained = batch_cnt_common_neis_merge
 
     # -- frontier algorithms --
@@ -443,6 +537,56 @@ class Partitioned_Graph:
         lab = _lib.as_array(labels, np.int32).copy()
         check(lib.pc_cdlp(self._pg, max_iterations, ptr(lab)))
         return lab
+
+
+class Batch:
+    """Many independent graphs in one arena, processed in one persistent
+    launch (pc_batch_* in include/pc.h).  Graph g owns arena vertices
+    [voff[g], voff[g+1])."""
+
+    TC, LCC, BFS = 1, 2, 4
+
+    def __init__(self, vlist, elist, voff):
+        self.vlist = _lib.as_array(vlist, np.uint64)
+        self.elist = _lib.as_array(elist, np.int32)
+        self.voff = _lib.as_array(voff, np.uint64)
+        out = C.c_void_p()
+        check(lib.pc_batch_create(ptr(self.vlist), ptr(self.elist), self.vlist.size - 1, self.elist.size,
+                                  ptr(self.voff), self.voff.size - 1, C.byref(out)))
+        self._b = out
+
+    @property
+    def num_graphs(self) -> int:
+        return int(self.voff.size - 1)
+
+    def run(self, tasks: int = 7):
+        n = self.vlist.size - 1
+        tc = np.zeros(self.num_graphs, np.uint64) if tasks & self.TC else None
+        lcc = np.zeros(n, np.float64) if tasks & self.LCC else None
+        bfs = np.zeros(n, np.int32) if tasks & self.BFS else None
+        st = _lib.BatchStats()
+        check(lib.pc_batch_run(self._b, tasks, ptr(tc), ptr(lcc), ptr(bfs), C.byref(st)))
+        return {"tc": tc, "lcc": lcc, "bfs": bfs, "ms": st.ms, "items": st.items, "threads": st.threads,
+                "ctas_per_sm": st.ctas_per_sm, "order": st.order}
+
+    def set_schedule(self, threads: int = 512, ctas_per_sm: int = 2, order: int = 0):
+        check(lib.pc_batch_set_schedule(self._b, threads, ctas_per_sm, order))
+
+    def autotune(self, tasks: int = 7):
+        st = _lib.BatchStats()
+        check(lib.pc_batch_autotune(self._b, tasks, C.byref(st)))
+        return {"ms": st.ms, "threads": st.threads, "ctas_per_sm": st.ctas_per_sm, "order": st.order}
+
+    def close(self):
+        if getattr(self, "_b", None):
+            lib.pc_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 from . import selector  # noqa: E402

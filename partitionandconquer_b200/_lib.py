@@ -59,6 +59,16 @@ class TCStats(C.Structure):
     ]
 
 
+class BatchStats(C.Structure):
+    _fields_ = [
+        ("ms", C.c_double),
+        ("items", C.c_uint32),
+        ("threads", C.c_int32),
+        ("ctas_per_sm", C.c_int32),
+        ("order", C.c_int32),
+    ]
+
+
 P = C.c_void_p
 i32, u32, i64, u64, f32, f64 = C.c_int32, C.c_uint32, C.c_int64, C.c_uint64, C.c_float, C.c_double
 PP = C.POINTER(C.c_void_p)
@@ -76,6 +86,15 @@ _SIG = {
     "pc_graph_destroy": (i32, [P]),
     "pc_graph_info": (i32, [P, P, P, P]),
     "pc_graph_stream": (P, [P]),
+    "pc_greedy_partition": (i32, [P, i32, u64, P]),
+    "pc_host_greedy_partition": (i32, [P, P, u64, i32, u64, P]),
+    "pc_friend_triangle": (i32, [P, i32, P, u64, P]),
+    "pc_square_count": (i32, [P, P]),
+    "pc_graph_from_edges": (i32, [P, P, u64, u64, u32, P, PP]),
+    "pc_graph_rmat": (i32, [u32, u32, u64, u32, PP]),
+    "pc_graph_er": (i32, [u32, u64, u64, u32, PP]),
+    "pc_graph_add_weights": (i32, [P, u64, i32]),
+    "pc_graph_download": (i32, [P, P, P, P]),
     "pc_partition": (i32, [P, P, PP]),
     "pc_pgraph_destroy": (i32, [P]),
     "pc_pgraph_info": (i32, [P, P, P, P]),
@@ -99,11 +118,18 @@ _SIG = {
     "pc_mis_hashed": (i32, [P, u64, P]),
     "pc_cdlp": (i32, [P, i32, P]),
     "pc_tc_count_noalloc": (i32, [P, P, u64, u64, P, P]),
+    "pc_batch_create": (i32, [P, P, u64, u64, P, u32, PP]),
+    "pc_batch_destroy": (i32, [P]),
+    "pc_batch_run": (i32, [P, u32, P, P, P, P]),
+    "pc_batch_set_schedule": (i32, [P, i32, i32, i32]),
+    "pc_batch_autotune": (i32, [P, u32, P]),
+    "pc_synth_rmat_batch": (i32, [u32, u32, u32, u32, u32, u64, PP, P]),
     "pc_tc_units": (i32, [P, P]),
     "pc_tc_unit_features": (i32, [P, P, i32]),
     "pc_tc_plan": (i32, [P, i32, P, i32]),
     "pc_tc_time_unit": (i32, [P, i32, i32, P, P]),
     "pc_selector_collect": (i32, [P, i32, i32, P]),
+    "pc_selector_collect_insitu": (i32, [P, i32, P]),
     "pc_selector_num_samples": (i32, []),
     "pc_selector_get_samples": (i32, [P, P, P, i32]),
     "pc_selector_add_samples": (i32, [P, P, P, i32]),

@@ -1,6 +1,7 @@
 // C ABI of the host-side helpers: seeded synthetic graphs and the reference's
 // binary CSR files.  Errors are reported through pc_last_error() like the
 // device entry points.
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
@@ -119,6 +120,33 @@ pc_status pc_host_csr_from_arrays(const uint64_t* vlist, const int32_t* elist, c
 pc_status pc_host_csr_free(pc_host_csr* g) {
     pc::clear_error();
     delete g;
+    return PC_OK;
+}
+
+pc_status pc_synth_rmat_batch(uint32_t G, uint32_t smin, uint32_t smax, uint32_t emin, uint32_t emax, uint64_t seed,
+                              pc_host_csr** out, uint64_t* voff) {
+    pc::clear_error();
+    if (!out || !voff || G == 0) return fail(PC_ERR_INVALID_INPUT, "bad argument");
+    if (smin < 1 || smax > 26 || smin > smax || emin < 1 || emin > emax)
+        return fail(PC_ERR_INVALID_INPUT, "bad scale or edge-factor range");
+    try {
+        std::vector<uint64_t> v;
+        pc_status st = wrap(pc::gen_rmat_batch(G, smin, smax, emin, emax, seed, &v), out);
+        if (st == PC_OK) memcpy(voff, v.data(), v.size() * 8);
+        return st;
+    } catch (const std::bad_alloc&) {
+        return fail(PC_ERR_OOM, "host allocation failed");
+    }
+}
+
+pc_status pc_host_greedy_partition(const uint64_t* vlist, const int32_t* elist, uint64_t n, int32_t P, uint64_t seed,
+                                   int32_t* v2p) {
+    pc::clear_error();
+    if (!vlist || (vlist[n] && !elist) || (n && !v2p)) return fail(PC_ERR_INVALID_INPUT, "null argument");
+    if (P < 1) return fail(PC_ERR_INVALID_INPUT, "partition count must be positive");
+    std::vector<int> out;
+    pc::greedy_partition_host(n, vlist, elist, (size_t)P, seed, out);
+    std::copy(out.begin(), out.end(), v2p);
     return PC_OK;
 }
 

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <fstream>
 #include <numeric>
+#include <random>
 
 #include "../synth_rng.h"
 
@@ -21,24 +22,29 @@ namespace {
 void exclusive_scan_u64(const std::vector<uint64_t>& counts, std::vector<uint64_t>& off) {
     const uint64_t n = counts.size();
     off.assign(n + 1, 0);
-    int nt = omp_get_max_threads();
+    const int nt = omp_get_max_threads();
     std::vector<uint64_t> part(nt + 1, 0);
+    int used = 1;
 #pragma omp parallel num_threads(nt)
     {
-        int t = omp_get_thread_num();
-        uint64_t lo = n * t / nt, hi = n * (t + 1) / nt, s = 0;
+        // the team can be smaller than nt (nested inside another parallel region)
+        const int T = omp_get_num_threads(), t = omp_get_thread_num();
+        uint64_t lo = n * t / T, hi = n * (t + 1) / T, s = 0;
         for (uint64_t i = lo; i < hi; ++i) s += counts[i];
         part[t + 1] = s;
 #pragma omp barrier
 #pragma omp single
-        for (int i = 0; i < nt; ++i) part[i + 1] += part[i];
+        {
+            used = T;
+            for (int i = 0; i < T; ++i) part[i + 1] += part[i];
+        }
         s = part[t];
         for (uint64_t i = lo; i < hi; ++i) {
             off[i] = s;
             s += counts[i];
         }
     }
-    off[n] = part[nt];
+    off[n] = part[used];
 }
 
 }  // namespace
@@ -178,6 +184,39 @@ HostCSR gen_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, bool degre
     return degree_relabel ? relabel_by_degree(g) : g;
 }
 
+HostCSR gen_rmat_batch(uint32_t G, uint32_t smin, uint32_t smax, uint32_t emin, uint32_t emax, uint64_t seed,
+                       std::vector<uint64_t>* voff) {
+    const uint64_t key = pc_graph_key(seed, PC_GEN_BATCH);
+    std::vector<HostCSR> gs(G);
+    // one graph per thread (the builders' own parallel regions run nested, serially)
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t g = 0; g < (int64_t)G; ++g) {
+        const uint32_t scale = smin + (uint32_t)(pc_draw(key, 2 * (uint64_t)g) % (uint64_t)(smax - smin + 1));
+        const uint32_t ef = emin + (uint32_t)(pc_draw(key, 2 * (uint64_t)g + 1) % (uint64_t)(emax - emin + 1));
+        gs[g] = gen_rmat(scale, ef, (uint64_t)g, true);
+    }
+    voff->assign(G + 1, 0);
+    std::vector<uint64_t> eoff(G + 1, 0);
+    for (uint32_t g = 0; g < G; ++g) {
+        (*voff)[g + 1] = (*voff)[g] + gs[g].n;
+        eoff[g + 1] = eoff[g] + gs[g].m;
+    }
+    HostCSR a;
+    a.n = (*voff)[G];
+    a.m = eoff[G];
+    a.vlist.resize(a.n + 1);
+    a.elist.resize(a.m);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t g = 0; g < (int64_t)G; ++g) {
+        const HostCSR& x = gs[g];
+        const uint64_t vb = (*voff)[g], eb = eoff[g];
+        for (uint64_t u = 0; u < x.n; ++u) a.vlist[vb + u] = eb + x.vlist[u];
+        for (uint64_t k = 0; k < x.m; ++k) a.elist[eb + k] = x.elist[k] + (int32_t)vb;
+    }
+    a.vlist[a.n] = a.m;
+    return a;
+}
+
 HostCSR gen_er(uint32_t scale, uint64_t nedges, uint64_t seed, bool degree_relabel) {
     const uint64_t n = 1ull << scale;
     const uint64_t key = pc_graph_key(seed, PC_GEN_ER);
@@ -309,6 +348,47 @@ bool load_csr_binfiles(const std::string& dir, bool weighted, HostCSR* g, std::s
     std::string e = validate_csr(g->n, g->m, g->vlist.data(), g->elist.data(), false);
     if (!e.empty()) { if (err) *err = e; return false; }
     return true;
+}
+
+
+void greedy_partition_host(uint64_t n, const uint64_t* vlist, const int32_t* elist, size_t P, uint64_t seed,
+                           std::vector<int>& v2p) {
+    // src/Graph.cpp:898-967 with one seeded engine in place of random_device
+    // and rand(), so the result is reproducible.
+    std::vector<std::pair<int32_t, int>> deg(n);
+    v2p.assign(n, -1);
+    for (uint64_t i = 0; i < n; ++i) deg[i] = {(int32_t)i, (int)(vlist[i + 1] - vlist[i])};
+    std::sort(deg.begin(), deg.end(),
+              [](std::pair<int32_t, int> a, std::pair<int32_t, int> b) { return a.second > b.second; });
+    std::mt19937 rng((uint32_t)seed);
+    std::vector<int> cnt(P);
+    std::vector<int32_t> free_nbrs;
+    std::vector<int> plist(P);
+    for (const auto& item : deg) {
+        std::fill(cnt.begin(), cnt.end(), 0);
+        free_nbrs.clear();
+        const int32_t u = item.first;
+        for (uint64_t i = vlist[u]; i < vlist[u + 1]; ++i) {
+            const int32_t v = elist[i];
+            if (v2p[v] > -1) cnt[v2p[v]]++;
+            else free_nbrs.push_back(v);
+        }
+        if (free_nbrs.empty()) continue;
+        std::shuffle(free_nbrs.begin(), free_nbrs.end(), rng);
+        const int ulb = item.second / (int)P;
+        for (size_t k = 0; k < P; ++k) plist[k] = std::max(0, ulb - cnt[k]);
+        const long long psum = std::accumulate(plist.begin(), plist.end(), 0LL);
+        size_t ptr = 0;
+        if (psum > 0) {
+            for (size_t k = 0; k < P; ++k) {
+                const size_t len = (size_t)((long long)plist[k] * (long long)free_nbrs.size() / psum);
+                for (size_t j = 0; j < len && ptr < free_nbrs.size(); ++j) v2p[free_nbrs[ptr++]] = (int)k;
+            }
+        }
+        for (; ptr < free_nbrs.size(); ++ptr) v2p[free_nbrs[ptr]] = (int)(rng() % P);
+    }
+    for (uint64_t u = 0; u < n; ++u)
+        if (v2p[u] == -1) v2p[u] = (int)(rng() % P);
 }
 
 }  // namespace pc

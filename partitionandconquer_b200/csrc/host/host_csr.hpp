@@ -37,6 +37,11 @@ HostCSR gen_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, bool degre
 HostCSR gen_er(uint32_t scale, uint64_t nedges, uint64_t seed, bool degree_relabel);
 HostCSR gen_chung_lu(uint32_t scale, uint64_t nedges, double beta, uint64_t dmax, uint64_t seed, bool degree_relabel);
 
+// G RMAT graphs packed in one arena (graph g: RMAT seed g; scale and edge
+// factor drawn from `seed`), each degree-relabelled; voff gets G+1 offsets.
+HostCSR gen_rmat_batch(uint32_t G, uint32_t smin, uint32_t smax, uint32_t emin, uint32_t emax, uint64_t seed,
+                       std::vector<uint64_t>* voff);
+
 // Raw edge streams (before symmetrisation), for the device-side builder tests.
 void rmat_edges(uint32_t scale, uint64_t nedges, uint64_t seed, uint32_t* src, uint32_t* dst);
 
@@ -46,6 +51,11 @@ void add_weights(HostCSR& g, uint64_t seed, int32_t wmax);
 // Validation of the boundary input: monotone offsets, ids in range, sorted
 // rows, weights length.  Returns an empty string when valid.
 std::string validate_csr(uint64_t n, uint64_t m, const uint64_t* vlist, const int32_t* elist, bool require_sorted);
+
+// Graph::greedy_partition (src/Graph.cpp:898-967) with a seeded engine in
+// place of random_device and rand().
+void greedy_partition_host(uint64_t n, const uint64_t* vlist, const int32_t* elist, size_t P, uint64_t seed,
+                           std::vector<int>& v2p);
 
 // Binary files in the reference format.
 bool save_csr_binfiles(const HostCSR& g, const std::string& dir, std::string* err);

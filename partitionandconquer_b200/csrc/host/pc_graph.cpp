@@ -22,8 +22,10 @@ static void check(pc_status s) {
 
 // ---- Graph: construction ---------------------------------------------------------
 
-Graph::Graph(const std::string graphfile) {
-    // src/Graph.cpp:27-90
+// The text loader's parse (src/Graph.cpp:27-57): '#'/'%' comment lines,
+// "u v" per line, self-loops skipped, ids shifted down by one unless a 0 id
+// appears.  Returns the vertex count and the shifted endpoint streams.
+static size_t parse_edge_text(const std::string& graphfile, std::vector<uint32_t>* s, std::vector<uint32_t>* d) {
     FILE* fp = fopen(graphfile.c_str(), "r");
     if (!fp) throw Error(PC_ERR_INVALID_INPUT, "cannot open " + graphfile);
     bool has_zero = false;
@@ -44,16 +46,45 @@ Graph::Graph(const std::string graphfile) {
         edges.emplace_back((VID)u, (VID)v);
     }
     fclose(fp);
-    vertex_num = maxid + (has_zero ? 1 : 0);
-    std::vector<uint32_t> s(edges.size()), d(edges.size());
+    s->resize(edges.size());
+    d->resize(edges.size());
     for (size_t i = 0; i < edges.size(); ++i) {
-        s[i] = (uint32_t)(edges[i].first - (has_zero ? 0 : 1));
-        d[i] = (uint32_t)(edges[i].second - (has_zero ? 0 : 1));
+        (*s)[i] = (uint32_t)(edges[i].first - (has_zero ? 0 : 1));
+        (*d)[i] = (uint32_t)(edges[i].second - (has_zero ? 0 : 1));
     }
-    HostCSR g = build_symmetric_csr(vertex_num, edges.size(), s.data(), d.data());
+    return maxid + (has_zero ? 1 : 0);
+}
+
+Graph::Graph(const std::string graphfile) {
+    // src/Graph.cpp:27-90
+    std::vector<uint32_t> s, d;
+    vertex_num = parse_edge_text(graphfile, &s, &d);
+    HostCSR g = build_symmetric_csr(vertex_num, s.size(), s.data(), d.data());
     csr_vlist.assign(g.vlist.begin(), g.vlist.end());
     csr_elist.assign(g.elist.begin(), g.elist.end());
     edge_num = csr_elist.size();
+}
+
+Graph::Graph(const std::string graphfile, OnDevice) {
+    // the same parse; the adjacency build (src/Graph.cpp:59-85) runs on the GPU
+    std::vector<uint32_t> s, d;
+    vertex_num = parse_edge_text(graphfile, &s, &d);
+    if (vertex_num == 0) return;
+    pc_graph* h = nullptr;
+    check(pc_graph_from_edges(s.data(), d.data(), s.size(), vertex_num, 0u, nullptr, &h));
+    uint64_t n = 0, m = 0;
+    int32_t w = 0;
+    pc_graph_info(h, &n, &m, &w);
+    csr_vlist.resize(n + 1);
+    csr_elist.resize(m);
+    const pc_status st = pc_graph_download(h, reinterpret_cast<uint64_t*>(csr_vlist.data()), csr_elist.data(), nullptr);
+    if (st != PC_OK) {
+        const std::string msg = pc_last_error();
+        pc_graph_destroy(h);
+        throw Error(st, msg);
+    }
+    edge_num = m;
+    dev_ = h;  // the CSR is already on the device
 }
 
 Graph::Graph(const std::string csrdir, bool is_weighted) {
@@ -172,47 +203,20 @@ void Graph::random_partition(const size_t part_num, std::vector<int>& v2p) {
 }
 
 void Graph::greedy_partition(const size_t P, std::vector<int>& v2p, uint64_t seed) {
-    // src/Graph.cpp:898-967 with one seeded engine in place of random_device
-    // and rand(), so the result is reproducible.
-    std::vector<std::pair<VID, int>> deg(vertex_num);
-    v2p.assign(vertex_num, -1);
-    for (size_t i = 0; i < vertex_num; ++i) deg[i] = {(VID)i, (int)get_deg((VID)i)};
-    std::sort(deg.begin(), deg.end(), [](std::pair<VID, int> a, std::pair<VID, int> b) { return a.second > b.second; });
-    std::mt19937 rng((uint32_t)seed);
-    std::vector<int> cnt(P);
-    std::vector<VID> free_nbrs;
-    std::vector<int> plist(P);
-    for (const auto& item : deg) {
-        std::fill(cnt.begin(), cnt.end(), 0);
-        free_nbrs.clear();
-        const VID u = item.first;
-        for (EID i = csr_vlist[u]; i < csr_vlist[u + 1]; ++i) {
-            const VID v = csr_elist[i];
-            if (v2p[v] > -1) cnt[v2p[v]]++;
-            else free_nbrs.push_back(v);
-        }
-        if (free_nbrs.empty()) continue;
-        std::shuffle(free_nbrs.begin(), free_nbrs.end(), rng);
-        const int ulb = item.second / (int)P;
-        for (size_t k = 0; k < P; ++k) plist[k] = std::max(0, ulb - cnt[k]);
-        const long long psum = std::accumulate(plist.begin(), plist.end(), 0LL);
-        size_t ptr = 0;
-        if (psum > 0) {
-            for (size_t k = 0; k < P; ++k) {
-                const size_t len = (size_t)((long long)plist[k] * (long long)free_nbrs.size() / psum);
-                for (size_t j = 0; j < len && ptr < free_nbrs.size(); ++j) v2p[free_nbrs[ptr++]] = (int)k;
-            }
-        }
-        for (; ptr < free_nbrs.size(); ++ptr) v2p[free_nbrs[ptr]] = (int)(rng() % P);
-    }
-    for (size_t u = 0; u < vertex_num; ++u)
-        if (v2p[u] == -1) v2p[u] = (int)(rng() % P);
+    greedy_partition_host(vertex_num, reinterpret_cast<const uint64_t*>(csr_vlist.data()), csr_elist.data(), P, seed,
+                          v2p);
 }
 
 // ---- Graph: algorithms (one partition) ------------------------------------------------
 
 size_t Graph::solve_triangle_counting_galloping(const int) const { return whole().solve_triangle_counting_galloping(); }
 size_t Graph::solve_triangle_counting_merge(const int) const { return whole().solve_triangle_counting_merge(); }
+size_t Graph::solve_friend_triangle_galloping(const VID root, const std::vector<VID>& nodes, const int) const {
+    return whole().solve_friend_triangle_galloping(root, nodes);
+}
+size_t Graph::solve_friend_triangle_merge(const VID root, const std::vector<VID>& nodes, const int) const {
+    return whole().solve_friend_triangle_merge(root, nodes);
+}
 void Graph::batch_cnt_common_neis_merge(const std::vector<std::pair<VID, VID>>& q, std::vector<size_t>& r, int) const {
     whole().batch_cnt_common_neis_merge(q, r);
 }
@@ -288,6 +292,22 @@ size_t Partitioned_Graph::solve_triangle_counting_merge() const {
     uint64_t c = 0;
     check(pc_tc(pg_, PC_METHOD_MERGE, &c));
     return (size_t)c;
+}
+
+size_t Partitioned_Graph::solve_friend_triangle_merge(const VID root, const std::vector<VID>& nodes) const {
+    uint64_t c = 0;
+    check(pc_friend_triangle(pg_, root, nodes.data(), nodes.size(), &c));
+    return c;
+}
+
+size_t Partitioned_Graph::solve_friend_triangle_galloping(const VID root, const std::vector<VID>& nodes) const {
+    return solve_friend_triangle_merge(root, nodes);
+}
+
+size_t Partitioned_Graph::solve_square_counting() const {
+    uint64_t c = 0;
+    check(pc_square_count(pg_, &c));
+    return c;
 }
 
 void Partitioned_Graph::batch_cnt_common_neis_merge(const std::vector<std::pair<VID, VID>>& q,

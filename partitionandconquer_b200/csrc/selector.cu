@@ -3,7 +3,10 @@
 // A small MLP (kMlpIn -> 64 -> 64 -> PC_NUM_VARIANTS, ReLU, fp32) predicts
 // log(milliseconds) of every TC kernel variant on a planning unit from the
 // unit's features.  Training data are timings the library measures itself
-// (pc_selector_collect runs each feasible variant on each unit alone).  The
+// (pc_selector_collect runs each feasible variant on each unit alone;
+// pc_selector_collect_insitu runs each variant on all units at once and
+// charges every unit its share of the run, measured by per-item cycle
+// counters -- the cost that matters when the units share the GPU).  The
 // network is trained on the GPU by the kernels below (forward, backward and
 // Adam in one single-CTA launch per training run); inference also runs on the
 // GPU.  The plain autotuned heuristic stays the fallback and the judge: the
@@ -543,6 +546,54 @@ pc_status pc_selector_collect(pc_pgraph* pg, int32_t max_units, int32_t repeats,
             msk[v] = 1;
         }
         std::lock_guard<std::mutex> lk(g_mu);
+        g_model.feats.insert(g_model.feats.end(), f, f + kNumFeatures);
+        g_model.logms.insert(g_model.logms.end(), logms, logms + kMlpOut);
+        g_model.mask.insert(g_model.mask.end(), msk, msk + kMlpOut);
+        ++n_added;
+    }
+    if (added) *added = n_added;
+    return PC_OK;
+}
+
+pc_status pc_selector_collect_insitu(pc_pgraph* pg, int32_t repeats, int32_t* added) {
+    clear_error();
+    if (!pg || repeats <= 0) return fail(PC_ERR_INVALID_INPUT, "bad argument");
+    PC_TRY(use_device(pg->g));
+    PC_TRY(tc_ensure_features(pg));
+    const size_t U = pg->unit_lo.size();
+    std::vector<std::vector<double>> best(kMlpOut, std::vector<double>(U, 1e30));
+    // counts agree among the variants that ran on the same units: the bitmap
+    // variants (ids within the bitmap) and the others (every unit with work)
+    uint64_t ref[2] = {0, 0};
+    bool have[2] = {false, false};
+    for (int v = 0; v < kMlpOut; ++v) {
+        const int cls = (v == PC_VARIANT_BITMAP_WARP || v == PC_VARIANT_BITMAP_GROUP8 || v == PC_VARIANT_BITMAP_LANE);
+        for (int r = 0; r < repeats; ++r) {
+            std::vector<double> ms;
+            uint64_t c = 0;
+            PC_TRY(tc_profile_variant(pg, v, &ms, &c));
+            if (!have[cls]) { ref[cls] = c; have[cls] = true; }
+            if (c != ref[cls]) {
+                char buf[160];
+                snprintf(buf, sizeof(buf), "variant %d counted %llu in a profiling run, expected %llu", v,
+                         (unsigned long long)c, (unsigned long long)ref[cls]);
+                return fail(PC_ERR_CUDA, buf);
+            }
+            for (size_t u = 0; u < U; ++u)
+                if (ms[u] >= 0) best[v][u] = std::min(best[v][u], ms[u]);
+        }
+    }
+    int32_t n_added = 0;
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (size_t u = 0; u < U; ++u) {
+        const float* f = &pg->part_features[u * kNumFeatures];
+        if (!(f[1] > 0 && f[2] > 0)) continue;
+        float logms[kMlpOut];
+        uint8_t msk[kMlpOut];
+        for (int v = 0; v < kMlpOut; ++v) {
+            msk[v] = best[v][u] < 1e29 ? 1 : 0;
+            logms[v] = msk[v] ? (float)std::log(std::max(best[v][u], 1e-6)) : 0.f;
+        }
         g_model.feats.insert(g_model.feats.end(), f, f + kNumFeatures);
         g_model.logms.insert(g_model.logms.end(), logms, logms + kMlpOut);
         g_model.mask.insert(g_model.mask.end(), msk, msk + kMlpOut);

@@ -36,7 +36,8 @@ PC_HD uint64_t pc_draw(uint64_t key, uint64_t counter) {
     return pc_mix64(key + counter * PC_GOLDEN_GAMMA);
 }
 
-enum { PC_GEN_RMAT = 1, PC_GEN_ER = 2, PC_GEN_CHUNG_LU = 3, PC_GEN_WEIGHT = 4, PC_GEN_PRIORITY = 5 };
+enum { PC_GEN_RMAT = 1, PC_GEN_ER = 2, PC_GEN_CHUNG_LU = 3, PC_GEN_WEIGHT = 4, PC_GEN_PRIORITY = 5, PC_GEN_BATCH = 6,
+       PC_GEN_PARTITION = 7 };
 
 // RMAT quadrant thresholds for (a, b, c, d) = (0.57, 0.19, 0.19, 0.05):
 // r < A -> (0,0); A <= r < AB -> column bit; AB <= r < ABC -> row bit; else both.

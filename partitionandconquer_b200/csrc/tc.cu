@@ -127,31 +127,40 @@ __device__ __forceinline__ int64_t range_pos(const int64_t* __restrict__ ranges,
     return ranges[2 * lo] + (int64_t)(q - (uint64_t)rprefix[lo]);
 }
 
-// Work items: per pivot ceil(din / chunk) items; pivots without a set or
-// without in-neighbours produce none.
+// Work items: pivot q (a linear position in the launch's position ranges)
+// gives ceil(din / chunk) items, each a run of <= chunk of its in-neighbours;
+// pivots without a set or without in-neighbours give none.
 __global__ void k_item_count(const uint64_t* __restrict__ off, const uint32_t* __restrict__ dplus,
                              const int32_t* __restrict__ plist, const int64_t* __restrict__ ranges,
                              const int64_t* __restrict__ rprefix, uint32_t nranges, uint64_t npos, uint32_t chunk,
                              uint32_t* __restrict__ cnt) {
-    const uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (q > npos) return;
-    if (q == npos) { cnt[q] = 0; return; }
-    const int32_t b = pivot_at(plist, range_pos(ranges, rprefix, nranges, q));
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t > npos) return;
+    if (t == npos) { cnt[t] = 0; return; }
+    const int32_t b = pivot_at(plist, range_pos(ranges, rprefix, nranges, t));
     const uint32_t dp = dplus[b];
-    const uint64_t din = off[b + 1] - off[b] - dp;
-    cnt[q] = (dp == 0 || din == 0) ? 0u : (uint32_t)((din + chunk - 1) / chunk);
+    const uint32_t din = (uint32_t)(off[b + 1] - off[b]) - dp;
+    cnt[t] = dp == 0 ? 0u : (din + chunk - 1) / chunk;
 }
 
-__global__ void k_item_fill(const int64_t* __restrict__ ranges, const int64_t* __restrict__ rprefix,
-                            uint32_t nranges, uint64_t npos, uint32_t chunk, const uint32_t* __restrict__ cnt,
-                            const uint32_t* __restrict__ start, Item* __restrict__ items) {
-    const uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (q >= npos) return;
-    const uint32_t c = cnt[q];
+__global__ void k_item_fill(const uint64_t* __restrict__ off, const uint32_t* __restrict__ dplus,
+                            const int32_t* __restrict__ plist, const int64_t* __restrict__ ranges,
+                            const int64_t* __restrict__ rprefix, uint32_t nranges, uint64_t npos, uint32_t chunk,
+                            const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ start,
+                            Item* __restrict__ items, uint32_t cap, uint32_t* __restrict__ nitems) {
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t == 0) *nitems = min(start[npos], cap);
+    if (t >= npos) return;
+    const uint32_t c = cnt[t];
     if (!c) return;
-    const int64_t p = range_pos(ranges, rprefix, nranges, q);
-    const uint32_t s = start[q];
-    for (uint32_t j = 0; j < c; ++j) items[s + j] = Item{(int32_t)p, (int32_t)(j * chunk)};
+    const int64_t p = range_pos(ranges, rprefix, nranges, t);
+    const int32_t b = pivot_at(plist, p);
+    const uint32_t din = (uint32_t)(off[b + 1] - off[b]) - dplus[b];
+    const uint32_t s = start[t];
+    for (uint32_t j = 0; j < c && s + j < cap; ++j) {
+        const uint32_t j0 = j * chunk;
+        items[s + j] = Item{(int32_t)p, (int32_t)j0, (int32_t)min(j0 + chunk, din)};
+    }
 }
 
 constexpr uint32_t kBitmapCapBits = 1u << 20;  // 128 KB of shared memory
@@ -190,13 +199,12 @@ static bool is_bitmap(int v) {
 
 // Bitmap sets per CTA: K warps share one set; the smallest K whose 16/K sets
 // fit the shared-memory budget (about 100 KB for two CTAs per SM, up to
-// 200 KB for one).  Items carry 256*K in-neighbours.
+// 200 KB for one).
 struct BitmapShape {
     int K;
     uint32_t words;
     size_t smem;
     int ctas_per_sm;
-    uint32_t chunk;
 };
 
 static BitmapShape bitmap_shape(uint32_t max_pivot_plus1) {
@@ -216,16 +224,17 @@ static BitmapShape bitmap_shape(uint32_t max_pivot_plus1) {
         sh.smem = (size_t)sh.words * 4;
     }
     sh.ctas_per_sm = (int)std::max<size_t>(1, std::min<size_t>(4, (220 * 1024) / (sh.smem + 1024)));
-    sh.chunk = 256u * (uint32_t)sh.K;
     return sh;
 }
 
 template <int K, int G>
 static pc_status launch_bitmap_kg(unsigned grid, size_t smem, cudaStream_t s, const uint64_t* off, const int32_t* adj,
                                   const uint32_t* dp, const int32_t* plist, const Item* items, const uint32_t* nitems,
-                                  uint32_t* next, unsigned long long* total, uint32_t words, uint32_t chunk) {
+                                  uint32_t* next, unsigned long long* total, uint32_t words, unsigned long long* cost,
+                                  const int32_t* unit_of) {
     PC_CUDA(cudaFuncSetAttribute(k_tc_bitmap<K, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_tc_bitmap<K, G><<<grid, kCtaThreads, smem, s>>>(off, adj, dp, plist, items, nitems, next, total, words, chunk);
+    k_tc_bitmap<K, G><<<grid, kCtaThreads, smem, s>>>(off, adj, dp, plist, items, nitems, next, total, words, cost,
+                                                      unit_of);
     return PC_OK;
 }
 
@@ -233,22 +242,25 @@ template <int K>
 static pc_status launch_bitmap_k(int G, unsigned grid, size_t smem, cudaStream_t s, const uint64_t* off,
                                  const int32_t* adj, const uint32_t* dp, const int32_t* plist, const Item* items,
                                  const uint32_t* nitems, uint32_t* next, unsigned long long* total, uint32_t words,
-                                 uint32_t chunk) {
-    if (G == 32) return launch_bitmap_kg<K, 32>(grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
-    if (G == 8) return launch_bitmap_kg<K, 8>(grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
-    return launch_bitmap_kg<K, 1>(grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
+                                 unsigned long long* cost, const int32_t* uo) {
+    if (G == 32)
+        return launch_bitmap_kg<K, 32>(grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
+    if (G == 8)
+        return launch_bitmap_kg<K, 8>(grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
+    return launch_bitmap_kg<K, 1>(grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
 }
 
 static pc_status launch_bitmap(int K, int G, unsigned grid, size_t smem, cudaStream_t s, const uint64_t* off,
                                const int32_t* adj, const uint32_t* dp, const int32_t* plist, const Item* items,
                                const uint32_t* nitems, uint32_t* next, unsigned long long* total, uint32_t words,
-                               uint32_t chunk) {
+                               unsigned long long* cost, const int32_t* uo) {
     switch (K) {
-        case 1: return launch_bitmap_k<1>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
-        case 2: return launch_bitmap_k<2>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
-        case 4: return launch_bitmap_k<4>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
-        case 8: return launch_bitmap_k<8>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
-        default: return launch_bitmap_k<16>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, chunk);
+        case 1: return launch_bitmap_k<1>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
+        case 2: return launch_bitmap_k<2>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
+        case 4: return launch_bitmap_k<4>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
+        case 8: return launch_bitmap_k<8>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
+        default:
+            return launch_bitmap_k<16>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
     }
 }
 
@@ -296,30 +308,51 @@ pc_status tc_ensure_features(pc_pgraph* pg) {
     return PC_OK;
 }
 
-// Launches one variant over the given position ranges (all asynchronous).
-static pc_status run_variant(pc_pgraph* pg, int v, const std::vector<int64_t>& ranges, uint64_t item_bound,
-                             uint32_t max_pivot_plus1, unsigned long long* d_total, uint64_t* launches) {
+// One launch: a variant and its bitmap shape (words rounded up to a power
+// of two).
+struct LaunchGroup {
+    int v = -1;
+    uint32_t words = 0;
+    std::vector<int64_t> ranges;
+    uint64_t npos = 0, item_bound = 0;
+    double ein = 0;
+    size_t units = 0;
+};
+
+// Items never exceed min(pivots, in-edges) + in-edges / chunk; the float
+// in-edge feature is widened by 256 per unit for its rounding.
+static void finish_group(LaunchGroup* gr) {
+    const uint64_t ein = (uint64_t)gr->ein + 256 * gr->units;
+    gr->item_bound = std::min<uint64_t>(gr->npos, ein) + ein / 256 + 1;
+}
+
+// Launches one group (all asynchronous).
+static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long long* d_total, uint64_t* launches,
+                           unsigned long long* d_cost) {
+    const int32_t* unit_of = pg->unit_of.as<int32_t>();
     cudaStream_t s = pg->g->stream;
+    const int v = gr.v;
     const uint32_t* dp = pg->dplus.as<uint32_t>();
     const int32_t* plist = pg->contiguous ? nullptr : pg->new2old.as<int32_t>();
     const int sms = sm_count(pg->g->device);
-    const uint32_t nr = (uint32_t)(ranges.size() / 2);
+    const uint32_t nr = (uint32_t)(gr.ranges.size() / 2);
     std::vector<int64_t> pref(nr + 1, 0);
-    for (uint32_t i = 0; i < nr; ++i) pref[i + 1] = pref[i] + (ranges[2 * i + 1] - ranges[2 * i]);
+    for (uint32_t i = 0; i < nr; ++i) pref[i + 1] = pref[i] + (gr.ranges[2 * i + 1] - gr.ranges[2 * i]);
     const uint64_t npos = (uint64_t)pref[nr];
     if (npos == 0) return PC_OK;
     int64_t* d_ranges = nullptr;
     int64_t* d_pref = nullptr;
-    PC_TRY(upload(pg, ranges.data(), ranges.size(), &d_ranges));
+    PC_TRY(upload(pg, gr.ranges.data(), gr.ranges.size(), &d_ranges));
     PC_TRY(upload(pg, pref.data(), nr + 1, &d_pref));
-    const uint32_t chunk = is_bitmap(v) ? bitmap_shape(max_pivot_plus1).chunk : (uint32_t)kChunkWarp;
+    const BitmapShape sh = bitmap_shape(gr.words * 32u);
+    const uint32_t chunk = is_bitmap(v) ? 256u * (uint32_t)sh.K : (uint32_t)kChunkWarp;
     uint32_t* d_cnt = pg->scratch.take<uint32_t>(npos + 1);
     uint32_t* d_start = pg->scratch.take<uint32_t>(npos + 1);
     size_t tmpb = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tmpb, d_cnt, d_start, (int64_t)(npos + 1), s);
     void* d_tmp = pg->scratch.take<char>(tmpb);
-    uint32_t* d_next = pg->scratch.take<uint32_t>(1);
-    Item* d_items = pg->scratch.take<Item>(item_bound);
+    uint32_t* d_next = pg->scratch.take<uint32_t>(2);
+    Item* d_items = pg->scratch.take<Item>(gr.item_bound);
     if (!d_cnt || !d_start || !d_tmp || !d_next || !d_items)
         return fail(PC_ERR_OOM, "scratch arena too small (internal sizing error)");
     k_item_count<<<(unsigned)ceil_div(npos + 1, 256), 256, 0, s>>>(pg->off, dp, plist, d_ranges, d_pref, nr, npos,
@@ -327,94 +360,139 @@ static pc_status run_variant(pc_pgraph* pg, int v, const std::vector<int64_t>& r
     PC_LAUNCHED();
     PC_CUDA(cub::DeviceScan::ExclusiveSum(d_tmp, tmpb, d_cnt, d_start, (int64_t)(npos + 1), s));
     count_launch();
-    k_item_fill<<<(unsigned)ceil_div(npos, 256), 256, 0, s>>>(d_ranges, d_pref, nr, npos, chunk, d_cnt, d_start,
-                                                              d_items);
+    k_item_fill<<<(unsigned)ceil_div(npos, 256), 256, 0, s>>>(pg->off, dp, plist, d_ranges, d_pref, nr, npos, chunk,
+                                                              d_cnt, d_start, d_items, (uint32_t)gr.item_bound,
+                                                              d_next + 1);
     PC_LAUNCHED();
     PC_CUDA(cudaMemsetAsync(d_next, 0, 4, s));
     *launches += 3;
-    const uint32_t* d_nitems = d_start + npos;
-    if (v == PC_VARIANT_BITMAP_WARP || v == PC_VARIANT_BITMAP_GROUP8 || v == PC_VARIANT_BITMAP_LANE) {
-        const BitmapShape sh = bitmap_shape(max_pivot_plus1);
+    const uint32_t* d_nitems = d_next + 1;
+    if (is_bitmap(v)) {
         const unsigned grid =
-            (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms * sh.ctas_per_sm, item_bound));
+            (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms * sh.ctas_per_sm, gr.item_bound));
         const int Gsel = v == PC_VARIANT_BITMAP_WARP ? 32 : (v == PC_VARIANT_BITMAP_GROUP8 ? 8 : 1);
         PC_TRY(launch_bitmap(sh.K, Gsel, grid, sh.smem, s, pg->off, pg->adj, dp, plist, d_items, d_nitems, d_next,
-                             d_total, sh.words, chunk));
+                             d_total, sh.words, d_cost, unit_of));
     } else {
         const unsigned grid = (unsigned)std::max<uint64_t>(
-            1, std::min<uint64_t>((uint64_t)sms * 8, ceil_div(item_bound, kWarpCtaWarps)));
+            1, std::min<uint64_t>((uint64_t)sms * 8, ceil_div(gr.item_bound, kWarpCtaWarps)));
         if (v == PC_VARIANT_HASH_WARP)
             k_tc_warp<kModeHash><<<grid, kWarpCtaWarps * 32, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems,
-                                                                     d_next, d_total);
+                                                                     d_next, d_total, d_cost, unit_of);
         else if (v == PC_VARIANT_MERGE_LANE)
             k_tc_warp<kModeMerge><<<grid, kWarpCtaWarps * 32, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems,
-                                                                      d_next, d_total);
+                                                                      d_next, d_total, d_cost, unit_of);
         else
             k_tc_warp<kModeGallop><<<grid, kWarpCtaWarps * 32, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems,
-                                                                       d_next, d_total);
+                                                                       d_next, d_total, d_cost, unit_of);
     }
     PC_LAUNCHED();
     *launches += 1;
     return PC_OK;
 }
 
-// Executes an assignment (one launch group per variant used) and returns the
-// count; the only host synchronisation is the final 8-byte read.
-static pc_status tc_execute(pc_pgraph* pg, const std::vector<int8_t>& assign, uint64_t* count, pc_tc_stats* stats) {
+// Executes an assignment (one launch group per variant and bitmap shape
+// used) and returns the count; the only host synchronisation is the final
+// 8-byte read.  With unit_ms (profiling runs) the kernels also charge their
+// warp-cycles to the units, every group is timed by its own events, and each
+// unit gets its group's time in proportion to its cycles: the unit's cost
+// inside a full run, where it shares the GPU with the other units.
+static pc_status tc_execute(pc_pgraph* pg, const std::vector<int8_t>& assign, uint64_t* count, pc_tc_stats* stats,
+                            std::vector<double>* unit_ms = nullptr) {
     cudaStream_t s = pg->g->stream;
     const std::vector<int64_t>& lo = pg->unit_lo;
     const std::vector<int64_t>& hi = pg->unit_hi;
     const std::vector<float>& feat = pg->part_features;
     const size_t U = lo.size();
-    // One launch group per variant; bitmap variants are further split by the
-    // shape (warps per bitmap set) their units' id ranges need, so hub units
-    // keep warp-private bitmaps.
-    struct Group {
-        int v = -1;
-        std::vector<int64_t> ranges;
-        uint64_t npos = 0, item_bound = 0;
-        uint32_t maxid = 0;
-    };
-    std::vector<Group> groups(PC_NUM_VARIANTS * 5);
+    // Bitmap units are grouped by their bitmap size rounded up to a power of
+    // two, so the hub units (small ids) get small sets and more CTAs per SM.
+    constexpr int kClasses = 16;
+    std::vector<LaunchGroup> groups(PC_NUM_VARIANTS * kClasses);
+    std::vector<int> group_of(U, -1);
     for (size_t u = 0; u < U; ++u) {
         const int v = assign[u];
         if (v < 0) continue;
         const uint32_t mid = (uint32_t)feat[u * kNumFeatures + 4];
-        int key = v * 5;
+        int c = 0;
         if (is_bitmap(v)) {
-            const int K = bitmap_shape(mid).K;
-            key += K == 1 ? 0 : K == 2 ? 1 : K == 4 ? 2 : K == 8 ? 3 : 4;
+            const uint32_t w = std::max<uint32_t>(1, (mid + 31) / 32);
+            while ((1u << c) < w && c < kClasses - 1) ++c;
         }
-        Group& gr = groups[key];
+        LaunchGroup& gr = groups[v * kClasses + c];
+        group_of[u] = v * kClasses + c;
         gr.v = v;
+        gr.words = 1u << c;
         if (!gr.ranges.empty() && gr.ranges.back() == lo[u]) gr.ranges.back() = hi[u];
         else { gr.ranges.push_back(lo[u]); gr.ranges.push_back(hi[u]); }
         gr.npos += (uint64_t)(hi[u] - lo[u]);
-        // items <= pivots + in-edges / 256 (the smallest chunk)
-        gr.item_bound += (uint64_t)(hi[u] - lo[u]) + (uint64_t)(feat[u * kNumFeatures + 1] / 256.0) + 1;
-        gr.maxid = std::max(gr.maxid, mid);
+        gr.ein += feat[u * kNumFeatures + 1];
+        gr.units += 1;
     }
     size_t need = 1024;
-    for (const Group& gr : groups) {
+    for (LaunchGroup& gr : groups) {
         if (gr.ranges.empty()) continue;
+        finish_group(&gr);
         size_t tmpb = 0;
-        cub::DeviceScan::ExclusiveSum(nullptr, tmpb, (uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t)(gr.npos + 1), s);
+        cub::DeviceScan::ExclusiveSum(nullptr, tmpb, (uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t)(gr.npos + 1),
+                                      s);
         need += gr.ranges.size() * 16 + 64 + (gr.npos + 1) * 8 + tmpb + gr.item_bound * sizeof(Item) + 8 * 256;
     }
+    if (unit_ms) need += U * 8 + 256;
     PC_TRY(scratch_reserve(pg, need));
     unsigned long long* d_total = pg->scratch.take<unsigned long long>(1);
+    unsigned long long* d_cost = unit_ms ? pg->scratch.take<unsigned long long>(std::max<size_t>(U, 1)) : nullptr;
+    std::vector<cudaEvent_t> gev;
+    auto drop_events = [&]() {
+        for (cudaEvent_t e : gev) cudaEventDestroy(e);
+        gev.clear();
+    };
+    if (unit_ms) {
+        gev.resize(2 * groups.size(), nullptr);
+        for (cudaEvent_t& e : gev)
+            if (cudaEventCreate(&e) != cudaSuccess) {
+                drop_events();
+                return fail(PC_ERR_CUDA, "event creation failed");
+            }
+        PC_CUDA(cudaMemsetAsync(d_cost, 0, std::max<size_t>(U, 1) * 8, s));
+    }
     uint64_t launches = 0;
     PC_CUDA(cudaEventRecord(pg->ev0, s));
     PC_CUDA(cudaMemsetAsync(d_total, 0, 8, s));
-    for (const Group& gr : groups) {
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const LaunchGroup& gr = groups[gi];
         if (gr.ranges.empty()) continue;
-        PC_TRY(run_variant(pg, gr.v, gr.ranges, gr.item_bound, gr.maxid, d_total, &launches));
+        if (unit_ms) PC_CUDA(cudaEventRecord(gev[2 * gi], s));
+        PC_TRY(run_group(pg, gr, d_total, &launches, d_cost));
+        if (unit_ms) PC_CUDA(cudaEventRecord(gev[2 * gi + 1], s));
     }
     PC_CUDA(cudaEventRecord(pg->ev1, s));
     unsigned long long h = 0;
     PC_CUDA(cudaMemcpyAsync(&h, d_total, 8, cudaMemcpyDeviceToHost, s));
-    PC_TRY(sync(pg));
+    std::vector<unsigned long long> cyc(unit_ms ? U : 0);
+    if (unit_ms && U) PC_CUDA(cudaMemcpyAsync(cyc.data(), d_cost, U * 8, cudaMemcpyDeviceToHost, s));
+    const pc_status st = sync(pg);
+    if (st != PC_OK) {
+        drop_events();
+        return st;
+    }
     *count = h;
+    if (unit_ms) {
+        unit_ms->assign(U, 0.0);
+        std::vector<double> gsum(groups.size(), 0.0), gms(groups.size(), 0.0);
+        for (size_t u = 0; u < U; ++u)
+            if (group_of[u] >= 0) gsum[group_of[u]] += (double)cyc[u];
+        for (size_t gi = 0; gi < groups.size(); ++gi) {
+            if (groups[gi].ranges.empty()) continue;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, gev[2 * gi], gev[2 * gi + 1]);
+            gms[gi] = ms;
+        }
+        for (size_t u = 0; u < U; ++u) {
+            const int gi = group_of[u];
+            if (gi >= 0 && gsum[gi] > 0) (*unit_ms)[u] = gms[gi] * (double)cyc[u] / gsum[gi];
+        }
+        drop_events();
+    }
     if (stats) {
         memset(stats, 0, sizeof(*stats));
         stats->partitions = pg->P;
@@ -485,6 +563,24 @@ pc_status tc_count(pc_pgraph* pg, int32_t variant, uint64_t* count, pc_tc_stats*
     PC_TRY(tc_assign(pg, variant, pg->part_features, U, &assign, &sel));
     PC_TRY(tc_execute(pg, assign, count, stats));
     if (stats) stats->selector = sel;
+    return PC_OK;
+}
+
+// Runs one variant on every unit it can take (all units with work; bitmap
+// variants only where the ids fit) in one profiled call; returns the per-unit
+// cost inside that full run, -1 where the variant cannot run, and the count
+// over the units it ran.
+pc_status tc_profile_variant(pc_pgraph* pg, int variant, std::vector<double>* unit_ms, uint64_t* count) {
+    PC_TRY(tc_ensure_features(pg));
+    const size_t U = pg->unit_lo.size();
+    std::vector<int8_t> assign(U, -1);
+    for (size_t u = 0; u < U; ++u) {
+        const float* f = &pg->part_features[u * kNumFeatures];
+        if (f[1] > 0 && f[2] > 0 && variant_feasible(variant, f)) assign[u] = (int8_t)variant;
+    }
+    PC_TRY(tc_execute(pg, assign, count, nullptr, unit_ms));
+    for (size_t u = 0; u < U; ++u)
+        if (assign[u] < 0) (*unit_ms)[u] = -1.0;
     return PC_OK;
 }
 

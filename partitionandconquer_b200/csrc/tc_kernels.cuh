@@ -12,7 +12,7 @@
 // count every triangle once.  Every kernel processes all in-edges of a set
 // of pivots, so kernels can be mixed per partition and the total stays exact.
 //
-// Work items are (pivot, chunk of in-neighbours) pairs taken from a global
+// Work items are (pivot, run of in-neighbours) triples taken from a global
 // counter, so hub pivots with 10^5 in-neighbours are spread over many CTAs.
 //
 // Pivot sets in shared memory:
@@ -28,7 +28,6 @@ namespace pc {
 namespace tc {
 
 constexpr int kTile = 16384;        // pivots per planning tile
-constexpr int kChunkCta = 2048;     // in-neighbours per CTA work item
 constexpr int kChunkWarp = 256;     // in-neighbours per warp work item
 constexpr int kCtaThreads = 512;    // threads per CTA of the bitmap kernels
 constexpr int kHashSlots = 512;     // slots per warp-private hash table
@@ -39,7 +38,8 @@ enum WarpMode { kModeHash = 0, kModeMerge = 1, kModeGallop = 2 };
 
 struct Item {
     int32_t pos;  // plist position of the pivot
-    int32_t j0;   // first in-neighbour (index into N-(b))
+    int32_t j0;   // in-neighbours [j0, j1) of the pivot (indices into N-(b))
+    int32_t j1;
 };
 
 __device__ __forceinline__ int32_t pivot_at(const int32_t* __restrict__ plist, int64_t p) {
@@ -98,8 +98,8 @@ __device__ __forceinline__ uint32_t scan_prefix_pipelined(const int32_t* __restr
 
 // Bitmap kernel: a CTA of kCtaThreads threads holds 16/K pivot bitmaps in
 // shared memory, one per group of K warps; each group takes its own work
-// items (pivot, <= 256*K in-neighbours), so a group synchronises only with
-// itself (a named barrier, or nothing when K == 1).  In-neighbour metadata
+// items (pivot, a run of its in-neighbours), so a group synchronises only
+// with itself (a named barrier, or nothing when K == 1).  In-neighbour metadata
 // (id, row offset, prefix length) is fetched 32 at a time with one coalesced
 // load and 32 independent gathers, then handed to groups of G lanes by
 // shuffles; each group scans one prefix with scan_prefix_pipelined.
@@ -112,7 +112,9 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
                                                            const uint32_t* __restrict__ nitems_p,
                                                            uint32_t* __restrict__ next_item,
                                                            unsigned long long* __restrict__ total,
-                                                           uint32_t bm_words, uint32_t chunk) {
+                                                           uint32_t bm_words,
+                                                           unsigned long long* __restrict__ unit_cost,
+                                                           const int32_t* __restrict__ unit_of) {
     extern __shared__ uint32_t smem[];
     __shared__ uint32_t s_item[16];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -136,6 +138,7 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
         set_sync();
         const uint32_t it = s_item[set];
         if (it >= nitems) break;
+        const long long t0 = unit_cost ? clock64() : 0;
         const Item I = items[it];
         const int32_t b = pivot_at(plist, I.pos);
         const uint64_t rb = off[b], re = off[b + 1];
@@ -146,7 +149,7 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
         }
         set_sync();
         const uint64_t in0 = rb + dp + (uint64_t)I.j0;
-        const uint64_t in1 = min(in0 + (uint64_t)chunk, re);
+        const uint64_t in1 = min(rb + dp + (uint64_t)I.j1, re);
         for (uint64_t base = in0 + (uint64_t)wi * 32; base < in1; base += (uint64_t)set_threads) {
             const uint64_t e = base + lane;
             const bool ok = e < in1;
@@ -168,6 +171,8 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
         set_sync();
         for (uint32_t k = tis; k < dp; k += set_threads) bm[adj[rb + k] >> 5] = 0;
         set_sync();
+        // profiling runs: the set's warp-cycles on this item, charged to its unit
+        if (unit_cost && tis == 0) atomicAdd(&unit_cost[unit_of[b]], (unsigned long long)(clock64() - t0) * K);
     }
     for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if (lane == 0 && cnt) atomicAdd(total, cnt);
@@ -220,7 +225,9 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
                                                                 const Item* __restrict__ items,
                                                                 const uint32_t* __restrict__ nitems_p,
                                                                 uint32_t* __restrict__ next_item,
-                                                                unsigned long long* __restrict__ total) {
+                                                                unsigned long long* __restrict__ total,
+                                                                unsigned long long* __restrict__ unit_cost,
+                                                                const int32_t* __restrict__ unit_of) {
     __shared__ int32_t table[MODE == kModeHash ? kWarpCtaWarps : 1][MODE == kModeHash ? kHashSlots : 1];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int32_t* T = table[MODE == kModeHash ? w : 0];
@@ -235,12 +242,13 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
         if (lane == 0) it = atomicAdd(next_item, 1u);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= nitems) break;
+        const long long t0 = unit_cost ? clock64() : 0;
         const Item I = items[it];
         const int32_t b = pivot_at(plist, I.pos);
         const uint64_t rb = off[b], re = off[b + 1];
         const uint32_t dp = dplus[b];
         const uint64_t in0 = rb + dp + (uint64_t)I.j0;
-        const uint64_t in1 = min(in0 + (uint64_t)kChunkWarp, re);
+        const uint64_t in1 = min(rb + dp + (uint64_t)I.j1, re);
         const int32_t* nb = adj + rb;
         if (MODE == kModeHash && dp <= (uint32_t)kHashCap) {
             for (uint32_t k = lane; k < dp; k += 32) {
@@ -277,6 +285,10 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
                 const int32_t c = adj[e];
                 cnt += merge_below(adj + off[c], dplus[c], nb, dp, b);
             }
+        }
+        if (unit_cost) {
+            __syncwarp();
+            if (lane == 0) atomicAdd(&unit_cost[unit_of[b]], (unsigned long long)(clock64() - t0));
         }
     }
     for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);

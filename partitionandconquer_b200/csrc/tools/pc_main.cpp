@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <fstream>
 #include <numeric>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -112,7 +113,10 @@ int run(int argc, char** argv) {
         // src/preprocess.cpp:39-45: text -> <dir>/origin CSR files + weights
         need(4);
         const string dir = argv[2], file = argv[3];
-        Graph g(dir + file);
+        // the adjacency build runs on the GPU when there is one (same arrays)
+        std::unique_ptr<Graph> gp = pc_device_count() > 0 ? std::make_unique<Graph>(dir + file, Graph::OnDevice{})
+                                                           : std::make_unique<Graph>(dir + file);
+        Graph& g = *gp;
         printf("Number of nodes: %d, number of edges: %llu.\n", g.get_vertex_num(), g.get_edge_num());
         g.save_as_csr_binfile(dir + "/origin/csr_vlist.bin", dir + "/origin/csr_elist.bin");
         g.add_reference_weights();

@@ -42,8 +42,17 @@ def time_unit(pg, unit: int, variant: int):
 
 
 def collect(pg, max_units: int = 256, repeats: int = 2) -> int:
+    """Each feasible variant timed on each sampled unit alone."""
     added = C.c_int32()
     check(lib.pc_selector_collect(pg.handle, max_units, repeats, C.byref(added)))
+    return int(added.value)
+
+
+def collect_insitu(pg, repeats: int = 2) -> int:
+    """Each variant run on all units at once; every unit charged its share
+    of the run (per-item cycle counters).  One sample per unit with work."""
+    added = C.c_int32()
+    check(lib.pc_selector_collect_insitu(pg.handle, repeats, C.byref(added)))
     return int(added.value)
 
 

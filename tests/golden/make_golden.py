@@ -121,6 +121,19 @@ def run_reference(name, vl, el, w, P):
         d["set_offsets"] = np.concatenate([[0], np.cumsum([len(s) for s in sets])]).astype(np.uint64)
         d["set_counts"] = R.batch_sets(sets)
         d["set_counts_partitioned"] = R.batch_sets(sets, partitioned=True)
+        # friend triangles around the highest-degree vertex (root and a repeat inside the list)
+        root = int(np.argmax(np.diff(vl.astype(np.int64))))
+        nodes = rng.integers(0, n, size=24).astype(np.int32)
+        nodes[3] = root
+        nodes[5] = nodes[4]
+        d["friend_root"] = np.int32(root)
+        d["friend_nodes"] = nodes
+        d["friend_merge"] = np.uint64(R.friend_triangle(root, nodes))
+        d["friend_galloping"] = np.uint64(R.friend_triangle(root, nodes, galloping=True))
+        d["friend_partitioned"] = np.uint64(R.friend_triangle(root, nodes, partitioned=True))
+        d["friend_partitioned_galloping"] = np.uint64(R.friend_triangle(root, nodes, partitioned=True,
+                                                                        galloping=True))
+        d["squares_partitioned"] = np.uint64(R.square_count())
     if n:
         d["bfs_levels"] = levels_from_parents(R.bfs_parents(0), 0)
         d["sssp"] = R.sssp(0)

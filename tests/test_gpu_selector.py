@@ -137,3 +137,33 @@ def test_selector_end_to_end_exact(gpu, O, tmp_path):
     assert st.selector == 1 and c == pgs[0][1]
     sel.enable(True)
     sel.clear()
+
+
+def test_insitu_collection_charges_every_unit(gpu, O):
+    """pc_selector_collect_insitu: one profiled full run per variant; every
+    unit with work gets a cost for each variant that can run it, the costs of
+    one run add up to that run's kernel time, and counts stay exact."""
+    pc = gpu
+    sel = pc.selector
+    sel.clear()
+    vl, el, _ = pc.HostCSR.rmat(16, 16, 2).arrays()
+    n = vl.size - 1
+    g = pc.Graph(vlist=vl, elist=el)
+    pg = pc.Partitioned_Graph(g, pc.equal_vertex_partition(n, 8))
+    feats = sel.unit_features(pg)
+    work = (feats[:, 1] > 0) & (feats[:, 2] > 0)
+    added = sel.collect_insitu(pg, repeats=1)
+    assert added == int(work.sum())
+    f, y, m = sel.samples()
+    assert f.shape[0] == added and m.any(axis=1).all()
+    # the warp variants (hash, merge, gallop) run on every unit with work
+    assert m[:, 3:].all()
+    assert np.isfinite(y[m.astype(bool)]).all()
+    # per-unit shares of the hash run add up to about one full hash-variant run
+    total = float(np.exp(y[:, 3]).sum())
+    c, st = pg.triangle_count(variant=pc.VARIANTS["hash_warp"], stats=True)
+    assert c == O.tc_merge(vl, el)
+    assert 0.2 * st.kernel_ms < total < 5.0 * st.kernel_ms
+    sel.clear()
+    pg.close()
+    g.close()

@@ -40,6 +40,10 @@ def test_oracle_matches_golden(O, name):
         sets = [d["set_ids"][offs[i]:offs[i + 1]] for i in range(offs.size - 1)]
         np.testing.assert_array_equal(O.batch_sets(vl, el, sets), d["set_counts"])
         np.testing.assert_array_equal(d["set_counts"], d["set_counts_partitioned"])
+        ft = O.friend_triangle(vl, el, int(d["friend_root"]), d["friend_nodes"])
+        assert ft == int(d["friend_merge"]) == int(d["friend_galloping"]) == int(d["friend_partitioned"]) \
+            == int(d["friend_partitioned_galloping"])
+        assert O.square_count(vl, el) == int(d["squares_partitioned"])
     if n:
         np.testing.assert_array_equal(O.bfs(vl, el, 0), d["bfs_levels"])
         # SSSP is pinned to the partitioned OpenMP path (exact shortest
@@ -105,6 +109,24 @@ def test_rmat16_generator_and_summary(pc, O):
     assert pr.sum() == pytest.approx(s["pagerank_f32_sum"], rel=1e-5)
 
 
+def partition_contiguous_ids(v2p):
+    """old -> new ids of Partitioned_Graph::reorder (src/Graph.cpp:1665-1699):
+    partition by partition, ascending original id inside a partition."""
+    order = np.lexsort((np.arange(v2p.size), v2p))
+    o2n = np.empty(v2p.size, np.int64)
+    o2n[order] = np.arange(v2p.size)
+    return o2n
+
+
+def relabel_csr(vl, el, o2n):
+    n = vl.size - 1
+    rows = np.repeat(np.arange(n), np.diff(vl).astype(np.int64))
+    key = np.sort(o2n[rows] * n + o2n[el.astype(np.int64)])
+    nvl = np.zeros(n + 1, np.uint64)
+    np.cumsum(np.bincount(key // n, minlength=n), out=nvl[1:])
+    return nvl, (key % n).astype(np.int32)
+
+
 @pytest.mark.parametrize("seed", [11, 12])
 def test_oracle_matches_live_reference(pc, O, seed):
     if not O.Reference.available():
@@ -133,9 +155,16 @@ def test_oracle_matches_live_reference(pc, O, seed):
         np.testing.assert_array_equal(R.mis(), O.mis(vl, el))
         lab = np.arange(n, dtype=np.int32)
         np.testing.assert_array_equal(R.cdlp(lab, 10, partitioned=True), O.cdlp(vl, el, lab, 10))
+        nodes = np.random.default_rng(seed).integers(0, n, 40).astype(np.int32)
+        assert R.friend_triangle(5, nodes, partitioned=True) == O.friend_triangle(vl, el, 5, nodes)
+        assert R.square_count() == O.square_count(vl, el)
         R.reorder()
         rv, re = R.layout()
         assert rv[-1] == el.size and re.size == el.size
+        # squares depend on the id order: after reorder() the reference counts
+        # in the partition-contiguous ids
+        nvl, nel = relabel_csr(vl, el, partition_contiguous_ids(v2p))
+        assert R.square_count() == O.square_count(nvl, nel)
     finally:
         R.close()
 
