@@ -1,5 +1,6 @@
 // Library plumbing of libpc.so: errors, device selection, graph upload with
 // device-side validation, the partitioned view, reorder and layout export.
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
@@ -235,6 +236,50 @@ __global__ void k_gather(const T* __restrict__ in, const int32_t* __restrict__ i
     if (i < n) out[i] = in[idx[i]];
 }
 
+// Partition vector checks: stats[0] |= 1 on a negative id, stats[1] = max
+// id, stats[2] |= 1 where v2p decreases (then partitions are not contiguous
+// id ranges).
+__global__ void k_v2p_stats(const int32_t* __restrict__ v2p, uint64_t n, int32_t* __restrict__ stats) {
+    int32_t mx = 0, neg = 0, dec = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n; u += stride) {
+        const int32_t k = v2p[u];
+        neg |= k < 0;
+        mx = max(mx, k);
+        if (u && k < v2p[u - 1]) dec = 1;
+    }
+    for (int o = 16; o; o >>= 1) {
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        neg |= __shfl_xor_sync(0xffffffffu, neg, o);
+        dec |= __shfl_xor_sync(0xffffffffu, dec, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (neg) atomicOr(&stats[0], 1);
+        atomicMax(&stats[1], mx);
+        if (dec) atomicOr(&stats[2], 1);
+    }
+}
+
+// pstart[k] = first position whose (non-decreasing) partition id is >= k.
+__global__ void k_partition_starts(const int32_t* __restrict__ key, uint64_t n, int64_t P, int64_t* __restrict__ pstart) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= n; i += stride) {
+        const int64_t cur = i < n ? key[i] : P;
+        const int64_t prev = i == 0 ? -1 : key[i - 1];
+        for (int64_t k = prev + 1; k <= cur; ++k) pstart[k] = (int64_t)i;
+    }
+}
+
+__global__ void k_iota_i32(int32_t* __restrict__ a, uint64_t n) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < n) a[i] = (int32_t)i;
+}
+
+__global__ void k_invert(const int32_t* __restrict__ new2old, uint64_t n, int32_t* __restrict__ old2new) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < n) old2new[new2old[i]] = (int32_t)i;
+}
+
 __global__ void k_map_ids(int32_t* ids, const int32_t* __restrict__ map, uint64_t count) {
     uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (i < count) ids[i] = map[ids[i]];
@@ -455,64 +500,89 @@ pc_status pc_partition(pc_graph* g, const int32_t* v2p, pc_pgraph** out) {
     *out = nullptr;
     PC_TRY(use_device(g));
     const uint64_t n = g->n;
-    int64_t maxp = 0;
-    bool contiguous = true;
-    if (v2p) {
-        for (uint64_t u = 0; u < n; ++u) {
-            int32_t k = v2p[u];
-            if (k < 0) return fail(PC_ERR_INVALID_INPUT, "partition ids must be non-negative");
-            if (k > maxp) maxp = k;
-            if (u && k < v2p[u - 1]) contiguous = false;
-        }
-    }
-    const int64_t P = maxp + 1;
-    if (P > (1 << 24)) return fail(PC_ERR_INVALID_INPUT, "more than 2^24 partitions");
+    cudaStream_t s = g->stream;
     pc_pgraph* pg = new pc_pgraph();
     pg->g = g;
-    pg->P = (int32_t)P;
-    pg->contiguous = contiguous;
     pg->off = g->off.as<uint64_t>();
     pg->adj = g->adj.as<int32_t>();
     pg->w = g->weighted ? g->w.as<int32_t>() : nullptr;
-    // poffsets / plist (src/Graph.cpp:1024-1035): vertices per partition, ascending id.
-    std::vector<int64_t> cnt(P + 1, 0);
-    for (uint64_t u = 0; u < n; ++u) cnt[(v2p ? v2p[u] : 0) + 1]++;
-    for (int64_t k = 0; k < P; ++k) cnt[k + 1] += cnt[k];
-    pg->pstart = cnt;
-    std::vector<int32_t> h_v2p;
-    pc_status st = PC_OK;
-    if (v2p) h_v2p.assign(v2p, v2p + n); else h_v2p.assign(n, 0);
-    if ((st = pg->v2p.alloc(std::max<uint64_t>(n, 1) * 4, "vertex2partition")) != PC_OK) { delete pg; return st; }
-    if ((st = pg->d_pstart.alloc((P + 1) * 8, "partition offsets")) != PC_OK) { delete pg; return st; }
-    cudaError_t e = cudaSuccess;
-    if (n) e = cudaMemcpyAsync(pg->v2p.p, h_v2p.data(), n * 4, cudaMemcpyHostToDevice, g->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(pg->d_pstart.p, pg->pstart.data(), (P + 1) * 8, cudaMemcpyHostToDevice, g->stream);
+    auto bail = [&](pc_status st) {
+        const std::string msg = pc_last_error();
+        cudaStreamSynchronize(s);
+        if (pg->ev0) cudaEventDestroy(pg->ev0);
+        if (pg->ev1) cudaEventDestroy(pg->ev1);
+        delete pg;
+        return fail(st, msg);
+    };
+    pc_status st;
+    if ((st = pg->v2p.alloc(std::max<uint64_t>(n, 1) * 4, "vertex2partition")) != PC_OK) return bail(st);
+    // checks, P = max + 1 (src/Graph.cpp:1021) and contiguity, on the device
+    int32_t stats[3] = {0, 0, 0};
+    if (v2p && n) {
+        DevBuf dstat;
+        if ((st = dstat.alloc(16, "partition checks")) != PC_OK) return bail(st);
+        cudaError_t e = cudaMemcpyAsync(pg->v2p.p, v2p, n * 4, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(dstat.p, 0, 16, s);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "partition upload", __FILE__, __LINE__));
+        k_v2p_stats<<<(unsigned)std::min<uint64_t>((uint64_t)sm_count(g->device) * 8, ceil_div(n, 256)), 256, 0, s>>>(
+            pg->v2p.as<int32_t>(), n, dstat.as<int32_t>());
+        count_launch();
+        e = cudaMemcpyAsync(stats, dstat.p, 12, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "partition checks", __FILE__, __LINE__));
+        if (stats[0]) return bail(fail(PC_ERR_INVALID_INPUT, "partition ids must be non-negative"));
+    } else if (n) {
+        if (cudaMemsetAsync(pg->v2p.p, 0, n * 4, s) != cudaSuccess)
+            return bail(fail(PC_ERR_CUDA, "memset of the partition vector failed"));
+    }
+    const int64_t P = (int64_t)stats[1] + 1;
+    if (P > (1 << 24)) return bail(fail(PC_ERR_INVALID_INPUT, "more than 2^24 partitions"));
+    const bool contiguous = stats[2] == 0;
+    pg->P = (int32_t)P;
+    pg->contiguous = contiguous;
+    if ((st = pg->d_pstart.alloc((P + 1) * 8, "partition offsets")) != PC_OK) return bail(st);
+    const unsigned nb = (unsigned)std::max<uint64_t>(1, ceil_div(n, 256));
+    const unsigned ng = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sm_count(g->device) * 16,
+                                                                           ceil_div(n + 1, 256)));
+    // poffsets / plist (src/Graph.cpp:1024-1035): vertices per partition, ascending id
+    if (contiguous) {
+        k_partition_starts<<<ng, 256, 0, s>>>(pg->v2p.as<int32_t>(), n, P, pg->d_pstart.as<int64_t>());
+        count_launch();
+    } else {
+        // plist = ids stably sorted by partition (an LSD radix sort is stable)
+        if ((st = pg->new2old.alloc(n * 4, "new2old")) != PC_OK || (st = pg->old2new.alloc(n * 4, "old2new")) != PC_OK)
+            return bail(st);
+        DevBuf keys, ids, tmp;
+        if ((st = keys.alloc(n * 4, "sort keys")) != PC_OK || (st = ids.alloc(n * 4, "sort values")) != PC_OK)
+            return bail(st);
+        int bits = 1;
+        while ((1ll << bits) < P) ++bits;
+        size_t tb = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, pg->v2p.as<int32_t>(), keys.as<int32_t>(), ids.as<int32_t>(),
+                                        pg->new2old.as<int32_t>(), (int64_t)n, 0, bits, s);
+        if ((st = tmp.alloc(std::max<size_t>(tb, 256), "sort scratch")) != PC_OK) return bail(st);
+        k_iota_i32<<<nb, 256, 0, s>>>(ids.as<int32_t>(), n);
+        count_launch();
+        cudaError_t e = cub::DeviceRadixSort::SortPairs(tmp.p, tb, pg->v2p.as<int32_t>(), keys.as<int32_t>(),
+                                                        ids.as<int32_t>(), pg->new2old.as<int32_t>(), (int64_t)n, 0,
+                                                        bits, s);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "partition sort", __FILE__, __LINE__));
+        count_launch();
+        k_invert<<<nb, 256, 0, s>>>(pg->new2old.as<int32_t>(), n, pg->old2new.as<int32_t>());
+        count_launch();
+        k_partition_starts<<<ng, 256, 0, s>>>(keys.as<int32_t>(), n, P, pg->d_pstart.as<int64_t>());
+        count_launch();
+        e = cudaStreamSynchronize(s);  // keys, ids and tmp are released on return
+        if (e != cudaSuccess) return bail(cuda_fail(e, "partition maps", __FILE__, __LINE__));
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return bail(cuda_fail(e, "kernel launch", __FILE__, __LINE__));
+    pg->pstart.assign(P + 1, 0);
+    e = cudaMemcpyAsync(pg->pstart.data(), pg->d_pstart.p, (P + 1) * 8, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaEventCreate(&pg->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&pg->ev1);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
-    if (e != cudaSuccess) {
-        delete pg;
-        return cuda_fail(e, "partition upload", __FILE__, __LINE__);
-    }
-    if (!contiguous) {
-        // plist: partition-major, ascending id within a partition.
-        std::vector<int32_t> plist(n);
-        std::vector<int64_t> cur(pg->pstart.begin(), pg->pstart.end() - 1);
-        for (uint64_t u = 0; u < n; ++u) plist[cur[h_v2p[u]]++] = (int32_t)u;
-        std::vector<int32_t> o2n(n);
-        for (uint64_t i = 0; i < n; ++i) o2n[plist[i]] = (int32_t)i;
-        if ((st = pg->new2old.alloc(n * 4, "new2old")) != PC_OK || (st = pg->old2new.alloc(n * 4, "old2new")) != PC_OK) {
-            delete pg;
-            return st;
-        }
-        e = cudaMemcpyAsync(pg->new2old.p, plist.data(), n * 4, cudaMemcpyHostToDevice, g->stream);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(pg->old2new.p, o2n.data(), n * 4, cudaMemcpyHostToDevice, g->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
-        if (e != cudaSuccess) {
-            delete pg;
-            return cuda_fail(e, "partition maps", __FILE__, __LINE__);
-        }
-    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "partition offsets", __FILE__, __LINE__));
     g->live_views++;
     *out = pg;
     return PC_OK;

@@ -156,8 +156,12 @@ __global__ void k_pr_init(const uint64_t* __restrict__ off, uint64_t n, T dampin
 }
 
 // One iteration: x'[v] = base + sum_{u in N(v)} contrib[u]; contrib'[v] = x'[v] / degs[v].
+// T is the storage type of the vectors; the row sums, x' and the division
+// run in fp64 for both instances, so the fp32 vectors carry only their own
+// storage rounding (within 1e-6 relative of the FP64 recurrence at 20
+// iterations; fp32 row sums over hub in-lists drift past that).
 template <class T>
-__global__ void k_pr_iter(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj, uint64_t n, T base,
+__global__ void k_pr_iter(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj, uint64_t n, double base,
                           const T* __restrict__ degs, const T* __restrict__ contrib, T* __restrict__ x_out,
                           T* __restrict__ contrib_out) {
     const int lane = threadIdx.x & 31;
@@ -165,14 +169,14 @@ __global__ void k_pr_iter(const uint64_t* __restrict__ off, const int32_t* __res
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t v = warp; v < n; v += nwarps) {
         const uint64_t b = off[v], e = off[v + 1];
-        T s = (T)0;
-        for (uint64_t j = b + lane; j < e; j += 32) s += __ldg(contrib + adj[j]);
+        double s = 0.0;
+        for (uint64_t j = b + lane; j < e; j += 32) s += (double)__ldg(contrib + adj[j]);
         for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0) {
-            const T x = base + s;
-            x_out[v] = x;
-            const T dg = degs[v];
-            contrib_out[v] = dg > (T)0 ? x / dg : (T)0;
+            const double x = base + s;
+            x_out[v] = (T)x;
+            const double dg = (double)degs[v];
+            contrib_out[v] = dg > 0.0 ? (T)(x / dg) : (T)0;
         }
     }
 }
@@ -402,8 +406,8 @@ static pc_status pagerank_run(pc_pgraph* pg, T damping, int32_t iters, const T* 
     }
     k_pr_init<T><<<nb, kThreads, 0, s>>>(pg->off, n, damping, ini, degs, c0);
     PC_LAUNCHED();
-    // (1 - damping) / n in the working precision (src/Graph.cpp:1558)
-    const T base = ((T)1 - damping) / (T)n;
+    // (1 - damping) / n (src/Graph.cpp:1558), in fp64 like the row sums
+    const double base = (1.0 - (double)damping) / (double)n;
     for (int32_t it = 0; it < iters; ++it) {
         k_pr_iter<T><<<grid_for(pg, 16), kThreads, 0, s>>>(pg->off, pg->adj, n, base, degs, c0, x, c1);
         PC_LAUNCHED();

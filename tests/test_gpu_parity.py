@@ -4,9 +4,9 @@ oracle and the reference's own golden outputs.
 Bars: integer results bit-exact; LCC / Jaccard bit-exact too (the integer
 numerators are exact and the division is one IEEE operation, as in the
 reference); PageRank fp64 within 1e-6 relative of the FP64 oracle (observed
-~1e-15); PageRank fp32 within 1e-4 relative (fp32 rounding of sums over up to
-10^4 terms; the reference's own fp32 run differs from FP64 by the same
-order)."""
+~1e-15); PageRank fp32 (fp32 vectors, fp64 row sums) within 1e-6 relative of
+the FP64 oracle too; against the reference's own fp32 run, whose fp32 row sums
+over up to 10^4 terms drift from FP64, within 1e-4."""
 from __future__ import annotations
 
 import numpy as np
@@ -17,7 +17,8 @@ from conftest import GOLDEN_GRAPHS, INT_MAX, golden_summary, load_golden, small_
 pytestmark = pytest.mark.gpu
 
 PR_F64_RTOL = 1e-6
-PR_F32_RTOL = 1e-4
+PR_F32_RTOL = 1e-6      # fp32 output against the FP64 oracle
+PR_F32_REF_RTOL = 1e-4  # fp32 output against the reference's fp32 output
 
 
 def partitions(n, rng):
@@ -245,7 +246,7 @@ def test_against_reference_golden(gpu, name):
         np.testing.assert_array_equal(pg.solve_mis(), d["mis"])
         np.testing.assert_array_equal(pg.solve_cdlp(np.arange(n, dtype=np.int32), 10), d["cdlp_partitioned"])
         np.testing.assert_allclose(pg.page_rank(0.85, 20).astype(np.float64),
-                                   d["pagerank_f32_partitioned"].astype(np.float64), rtol=PR_F32_RTOL, atol=0)
+                                   d["pagerank_f32_partitioned"].astype(np.float64), rtol=PR_F32_REF_RTOL, atol=0)
 
 
 def test_config1_rmat16(gpu, O):
