@@ -110,10 +110,17 @@ class Dist:
 
 # ---- workload -------------------------------------------------------------------
 
-def make_graph(pc, scale, ef, seed):
+def make_graph(pc, scale, ef, seed, device=False):
+    """The seeded RMAT graph: generated and built on the GPU (pc_graph_rmat)
+    for our arm, by the host generator (the same arrays) for the reference
+    arm, which runs none of the library's GPU code."""
     t = time.time()
-    h = pc.HostCSR.rmat(scale, ef, seed)
-    vl, el, _ = h.arrays()
+    if device:
+        g = pc.Graph.rmat_device(scale, ef, seed)
+        vl, el = g.get_csr_vlist(), g.get_csr_elist()
+        g.close()
+    else:
+        vl, el, _ = pc.HostCSR.rmat(scale, ef, seed).arrays()
     return vl, el, time.time() - t
 
 
@@ -265,26 +272,31 @@ def run_reference_arm(args, dist):
 
 def train_selector(pc, args):
     """Training data generated by the method itself on separate graphs (RMAT
-    seed 2 at the training scale, ER and Chung-Lu): per-unit timings of every
-    variant; then the MLP is trained on the GPU and the heuristic autotuned on
-    the same samples."""
+    at two scales with other seeds, ER and Chung-Lu): in-situ per-unit costs
+    of every variant, one collection group per graph; the heuristic is
+    autotuned on the samples, then the MLP is trained on the GPU with its
+    judge margin chosen by leave-one-graph-out validation."""
     sel = pc.selector
     sel.clear()
     s = args.train_scale
-    graphs = [pc.HostCSR.rmat(s, args.edge_factor, args.seed + 1),
-              pc.HostCSR.er(s - 2, 1 << (s + 2), args.seed + 2),
-              pc.HostCSR.chung_lu(s - 2, 1 << (s + 2), 2.1, 1 << (s - 6), args.seed + 3)]
-    for h in graphs:
-        vl, el, _ = h.arrays()
-        n = vl.size - 1
-        g = pc.Graph(vlist=vl, elist=el)
+    graphs = [lambda: pc.Graph.rmat_device(s - 2, args.edge_factor, args.seed + 4),
+              lambda: pc.Graph.rmat_device(s, args.edge_factor, args.seed + 1),
+              lambda: pc.Graph.rmat_device(s + 1, args.edge_factor, args.seed + 5),
+              lambda: pc.Graph.er_device(s - 2, 1 << (s + 2), args.seed + 2),
+              lambda: pc.Graph(host=pc.HostCSR.chung_lu(s - 2, 1 << (s + 2), 2.1, 1 << (s - 6), args.seed + 3))]
+    for make in graphs:
+        g = make()
+        n = g.get_vertex_num()
         pg = pc.Partitioned_Graph(g, pc.equal_vertex_partition(n, max(1, n // 16384)))
         sel.collect_insitu(pg, repeats=2)
         pg.close()
         g.close()
     tuned = sel.autotune()
     loss = sel.train(steps=1500, lr=3e-3, seed=7)
+    margin, gain = sel.judge()
     return {"samples": sel.num_samples(), "train_loss": loss, "heuristic_params": tuned.tolist(),
+            "judge_margin": None if not np.isfinite(margin) else round(float(np.exp(margin)), 4),
+            "heldout_gain_vs_plain": round(gain, 4),
             "collection": "in-situ: every variant run on all units at once, each unit charged its cycle share"}
 
 
@@ -335,7 +347,7 @@ def run_ours(args, dist):
     _lib.check(_lib.lib.pc_set_device(dev))
     if dist.world > 1:
         os.environ.setdefault("OMP_NUM_THREADS", str(max(1, (os.cpu_count() or 1) // dist.world)))
-    vl, el, t_gen = make_graph(pc, args.scale, args.edge_factor, args.seed)
+    vl, el, t_gen = make_graph(pc, args.scale, args.edge_factor, args.seed, device=True)
     n = vl.size - 1
     algo_bytes, W, e_plus = tc_algorithmic_bytes(vl, el)
     v2p = pc.equal_vertex_partition(n, args.partitions)
@@ -392,12 +404,16 @@ def run_ours(args, dist):
     for a in (vl, el, v2p):
         L.check(L.lib.pc_host_register(L.ptr(a), a.nbytes))
         pinned.append(a)
-    e2e = []
+    e2e, phases = [], []
     for i in range(args.e2e_steps + 1):
         t = time.perf_counter()
         g2 = pc.Graph(vlist=vl, elist=el)
+        g2._device()  # upload + device validation
+        t1 = time.perf_counter()
         pg2 = pc.Partitioned_Graph(g2, v2p)
-        c = pg2.triangle_count(variant=pc.VARIANT_AUTO)
+        t2 = time.perf_counter()
+        c = pg2.triangle_count(variant=pc.VARIANT_AUTO)  # features, plan, count, 8-byte read
+        t3 = time.perf_counter()
         pg2.close()
         g2.close()
         dt = time.perf_counter() - t
@@ -405,6 +421,7 @@ def run_ours(args, dist):
             raise SystemExit("e2e count mismatch")
         if i > 0:
             e2e.append(dt)
+            phases.append((t1 - t, t2 - t1, t3 - t2, dt - (t3 - t)))
     for a in pinned:
         L.lib.pc_host_unregister(L.ptr(a))
     bounds = plan_bounds(pc, pg)
@@ -442,7 +459,9 @@ def run_ours(args, dist):
                                  "plain_variants_per_unit": list(st_plain.variant_hist),
                                  "unit_cost_sums": bounds, **train},
             "e2e": {"value": round(e2e_value, 4), "unit": "GTEPS", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": 8, "ms_per_step": round(e2e_s * 1e3, 2)},
+                    "d2h_bytes_per_step": 8, "ms_per_step": round(e2e_s * 1e3, 2),
+                    "phases_ms": dict(zip(("upload_validate", "partition_view", "features_plan_count", "release"),
+                                          (round(statistics.median(x) * 1e3, 2) for x in zip(*phases))))},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                          "algorithmic_bytes": int(algo_bytes), "W": int(W), "kernel_ms": round(kernel_ms, 4)},

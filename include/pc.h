@@ -57,6 +57,10 @@ int32_t pc_device_count(void);
 pc_status pc_set_device(int32_t device);
 /* Total number of kernels this library has launched in this process. */
 uint64_t pc_launch_count(void);
+/* Device memory freed by the library stays cached in each device's
+ * stream-ordered pool for reuse by later handles; this returns it to the
+ * device.  Call it with no handle in use. */
+pc_status pc_release_cached_memory(void);
 /* Page-lock (or release) a caller buffer so host<->device copies are DMA. */
 pc_status pc_host_register(void* ptr, size_t bytes);
 pc_status pc_host_unregister(void* ptr);
@@ -160,7 +164,10 @@ pc_status pc_pgraph_evaluate(pc_pgraph* pg, int64_t* max_part_deg, int64_t* max_
 #define PC_VARIANT_HASH_WARP 3   /* warp-private pivot hash, lane per in-nbr     */
 #define PC_VARIANT_MERGE_LANE 4  /* threshold merge, lane per edge (reference)   */
 #define PC_VARIANT_GALLOP_LANE 5 /* binary search, lane per edge                 */
-#define PC_NUM_VARIANTS 6
+#define PC_VARIANT_MATRIX 6      /* hub units (ids < 2^16, contiguous partitions):
+                                    pivot bitmap rows resident in L2, in-neighbour
+                                    major, word-AND/popcount or bit probes       */
+#define PC_NUM_VARIANTS 7
 
 typedef struct {
     double kernel_ms;      /* device time of the intersection kernels (CUDA events) */
@@ -321,12 +328,21 @@ pc_status pc_selector_get_samples(float* feats, float* log_ms, uint8_t* mask, in
 pc_status pc_selector_add_samples(const float* feats, const float* log_ms, const uint8_t* mask, int32_t count);
 /* Train the MLP on the GPU (full batch, Adam) on the collected samples. */
 pc_status pc_selector_train(int32_t steps, float lr, uint64_t seed, float* final_loss);
+/* The judge chosen at training: the learned choice replaces the heuristic's
+ * only when predicted faster by more than exp(log_margin) (+inf: never), the
+ * margin with the lowest measured total on held-out collection groups
+ * (leave-one-group-out); heldout_gain = heuristic total / judged total there
+ * (0 when fewer than two groups were collected). */
+pc_status pc_selector_judge(double* log_margin, double* heldout_gain);
 /* Predicted log(ms) per variant for raw unit features. */
 pc_status pc_selector_predict(const float* feats, int32_t count, float* log_ms);
 /* Grid-search the heuristic's thresholds on the collected samples. */
-pc_status pc_selector_autotune(double* tuned /* 3 */);
-pc_status pc_selector_get_heuristic(double* params /* 3 */);
-pc_status pc_selector_set_heuristic(const double* params /* 3 */);
+pc_status pc_selector_autotune(double* tuned /* 4 */);
+/* Heuristic thresholds: in-edges per pivot for a shared-memory or resident
+ * bitmap form; mean prefix length for 32 lanes, for 8 lanes, and for the
+ * matrix form (1e30 = never). */
+pc_status pc_selector_get_heuristic(double* params /* 4 */);
+pc_status pc_selector_set_heuristic(const double* params /* 4 */);
 pc_status pc_selector_clear(void);
 int32_t pc_selector_trained(void);
 /* on == 0 makes PC_VARIANT_AUTO use the heuristic even when trained. */

@@ -36,10 +36,11 @@ VARIANTS = {
     "hash_warp": 3,
     "merge_lane": 4,
     "gallop_lane": 5,
+    "matrix": 6,
 }
-NUM_VARIANTS = 6
+NUM_VARIANTS = 7
 SELECTOR_FEATURES = 10
-MLP_IN, MLP_HIDDEN, MLP_OUT = 12, 64, 6
+MLP_IN, MLP_HIDDEN, MLP_OUT = 12, 64, NUM_VARIANTS
 
 
 class PCError(RuntimeError):
@@ -81,6 +82,7 @@ _SIG = {
     "pc_set_device": (i32, [i32]),
     "pc_launch_count": (u64, []),
     "pc_host_register": (i32, [P, C.c_size_t]),
+    "pc_release_cached_memory": (i32, []),
     "pc_host_unregister": (i32, [P]),
     "pc_graph_create": (i32, [P, P, P, u64, u64, u32, PP]),
     "pc_graph_destroy": (i32, [P]),
@@ -130,6 +132,7 @@ _SIG = {
     "pc_tc_time_unit": (i32, [P, i32, i32, P, P]),
     "pc_selector_collect": (i32, [P, i32, i32, P]),
     "pc_selector_collect_insitu": (i32, [P, i32, P]),
+    "pc_selector_judge": (i32, [P, P]),
     "pc_selector_num_samples": (i32, []),
     "pc_selector_get_samples": (i32, [P, P, P, i32]),
     "pc_selector_add_samples": (i32, [P, P, P, i32]),

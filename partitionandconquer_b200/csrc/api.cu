@@ -35,10 +35,37 @@ void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 // ---- memory ----------------------------------------------------------------
 
+// Device buffers come from the device's default stream-ordered memory pool,
+// whose release threshold is raised once per device so that freed blocks stay
+// cached in the process: creating and destroying graph handles again and
+// again (one upload per call of a drop-in caller) then reuses memory instead
+// of mapping and unmapping it each time.  pc_release_cached_memory() trims the
+// pools.  An allocation completes before alloc() returns (the legacy stream
+// is synchronised), and release() waits for the device to go idle before the
+// block returns to the pool, so no stream still uses it.
+static std::mutex g_pool_mu;
+static std::vector<int> g_pool_ready;
+
+static cudaError_t prepare_pool(int dev) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if ((int)g_pool_ready.size() <= dev) g_pool_ready.resize(dev + 1, 0);
+    if (g_pool_ready[dev]) return cudaSuccess;
+    cudaMemPool_t pool;
+    cudaError_t e = cudaDeviceGetDefaultMemPool(&pool, dev);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = ~0ull;
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e == cudaSuccess) g_pool_ready[dev] = 1;
+    return e;
+}
+
 pc_status DevBuf::alloc(size_t nbytes, const char* what) {
     release();
     if (nbytes == 0) return PC_OK;
-    cudaError_t e = cudaMalloc(&p, nbytes);
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = prepare_pool(dev);
+    if (e == cudaSuccess) e = cudaMallocAsync(&p, nbytes, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) {
         p = nullptr;
         cudaGetLastError();
@@ -54,7 +81,15 @@ pc_status DevBuf::ensure(size_t nbytes, const char* what) {
     return alloc(nbytes, what);
 }
 void DevBuf::release() {
-    if (p) cudaFree(p);
+    if (p) {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (cur != dev) cudaSetDevice(dev);
+        cudaDeviceSynchronize();
+        cudaFreeAsync(p, 0);
+        cudaStreamSynchronize(0);
+        if (cur != dev && cur >= 0) cudaSetDevice(cur);
+    }
     p = nullptr;
     bytes = 0;
 }
@@ -355,6 +390,24 @@ using namespace pc;
 extern "C" {
 
 const char* pc_last_error(void) { return g_last_error.c_str(); }
+
+pc_status pc_release_cached_memory(void) {
+    clear_error();
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    for (int d = 0; d < (int)g_pool_ready.size(); ++d) {
+        if (!g_pool_ready[d]) continue;
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, d) != cudaSuccess) continue;
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(d);
+        cudaDeviceSynchronize();
+        const cudaError_t e = cudaMemPoolTrimTo(pool, 0);
+        cudaSetDevice(cur);
+        if (e != cudaSuccess) return cuda_fail(e, "memory pool trim", __FILE__, __LINE__);
+    }
+    return PC_OK;
+}
 const char* pc_version(void) { return "pc-b200 0.1 (sm_100a)"; }
 
 int32_t pc_device_count(void) {

@@ -45,6 +45,7 @@ void count_launch();
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    int dev = 0;  // device whose pool holds the block
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;

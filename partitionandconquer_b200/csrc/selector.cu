@@ -272,11 +272,23 @@ struct Model {
     std::vector<float> params;       // kMlpParams
     float mean[kMlpIn] = {0}, stdv[kMlpIn] = {0};
     float lo[kMlpIn] = {0}, hi[kMlpIn] = {0};  // training range (standardised)
+    // The judge: the learned choice replaces the heuristic's only when it is
+    // predicted faster by more than this (log ratio).  Chosen by
+    // leave-one-group-out validation at training; +inf keeps the heuristic.
+    float judge_log_margin = 0.0487902f;  // log(1.05) until validated
+    double heldout_gain = 0.0;            // plain / judged cost on held-out groups (0: not validated)
     // samples
     std::vector<float> feats;   // kNumFeatures per sample (raw)
     std::vector<float> logms;   // kMlpOut per sample
     std::vector<uint8_t> mask;  // kMlpOut per sample
+    std::vector<int32_t> group; // one id per collection call (validation folds)
+    int32_t next_group = 0;
 };
+
+// Per-sample work scale: the model predicts log(ms) - log(1 + in-edges +
+// prefix ids), the cost per unit of work, so units of other sizes than the
+// training units stay comparable.  It cancels in the per-unit argmin.
+static float log_work(const float* f) { return (float)std::log(1.0 + (double)f[1] + (double)f[5]); }
 static Model g_model;
 
 static size_t train_smem_bytes() { return sizeof(TrainSmem) + 16; }
@@ -355,8 +367,9 @@ void bump_version_locked() { ++g_version; }
 
 // Learned choices, judged against the heuristic: for a unit the model must be
 // inside its training range (with a margin) and predict the heuristic's
-// choice at least 5% slower than its own; otherwise the heuristic's choice
-// stands.
+// choice slower than its own by more than the validated judge margin;
+// otherwise the heuristic's choice stands.  (The per-unit work scale of the
+// predictions cancels in these comparisons.)
 pc_status selector_choose_batch(const std::vector<float>& feat, size_t U, std::vector<int8_t>* choice) {
     Model md;
     {
@@ -367,9 +380,11 @@ pc_status selector_choose_batch(const std::vector<float>& feat, size_t U, std::v
         memcpy(md.stdv, g_model.stdv, sizeof(md.stdv));
         memcpy(md.lo, g_model.lo, sizeof(md.lo));
         memcpy(md.hi, g_model.hi, sizeof(md.hi));
+        md.judge_log_margin = g_model.judge_log_margin;
     }
     const HeuristicParams hp = heuristic_params();
     choice->assign(U, -1);
+    const bool use_model = std::isfinite(md.judge_log_margin);  // +inf: validation kept the heuristic
     std::vector<size_t> idx;
     std::vector<float> X;
     for (size_t u = 0; u < U; ++u) {
@@ -384,7 +399,7 @@ pc_status selector_choose_batch(const std::vector<float>& feat, size_t U, std::v
             const float span = md.hi[k] - md.lo[k];
             if (x[k] < md.lo[k] - 0.25f * span - 0.5f || x[k] > md.hi[k] + 0.25f * span + 0.5f) inside = false;
         }
-        if (!inside) continue;
+        if (!inside || !use_model) continue;
         idx.push_back(u);
         X.insert(X.end(), x, x + kMlpIn);
     }
@@ -399,7 +414,7 @@ pc_status selector_choose_batch(const std::vector<float>& feat, size_t U, std::v
         int best = -1;
         for (int v = 0; v < kMlpOut; ++v)
             if (tc::variant_feasible(v, f) && (best < 0 || y[v] < y[best])) best = v;
-        if (best >= 0 && y[h] - y[best] > std::log(1.05f)) (*choice)[u] = (int8_t)best;
+        if (best >= 0 && y[h] - y[best] > md.judge_log_margin) (*choice)[u] = (int8_t)best;
     }
     return PC_OK;
 }
@@ -518,6 +533,7 @@ pc_status pc_selector_collect(pc_pgraph* pg, int32_t max_units, int32_t repeats,
         for (size_t i = 0; i < want; ++i) pick.push_back(work[head + i * rest / want]);
     }
     int32_t n_added = 0;
+    int32_t gid = -1;
     for (size_t u : pick) {
         const float* f = &pg->part_features[u * kNumFeatures];
         float logms[kMlpOut];
@@ -546,9 +562,11 @@ pc_status pc_selector_collect(pc_pgraph* pg, int32_t max_units, int32_t repeats,
             msk[v] = 1;
         }
         std::lock_guard<std::mutex> lk(g_mu);
+        if (gid < 0) gid = g_model.next_group++;
         g_model.feats.insert(g_model.feats.end(), f, f + kNumFeatures);
         g_model.logms.insert(g_model.logms.end(), logms, logms + kMlpOut);
         g_model.mask.insert(g_model.mask.end(), msk, msk + kMlpOut);
+        g_model.group.push_back(gid);
         ++n_added;
     }
     if (added) *added = n_added;
@@ -563,11 +581,15 @@ pc_status pc_selector_collect_insitu(pc_pgraph* pg, int32_t repeats, int32_t* ad
     const size_t U = pg->unit_lo.size();
     std::vector<std::vector<double>> best(kMlpOut, std::vector<double>(U, 1e30));
     // counts agree among the variants that ran on the same units: the bitmap
-    // variants (ids within the bitmap) and the others (every unit with work)
-    uint64_t ref[2] = {0, 0};
-    bool have[2] = {false, false};
+    // variants (ids within the bitmap), the matrix form (ids below 2^16) and
+    // the others (every unit with work)
+    uint64_t ref[3] = {0, 0, 0};
+    bool have[3] = {false, false, false};
     for (int v = 0; v < kMlpOut; ++v) {
-        const int cls = (v == PC_VARIANT_BITMAP_WARP || v == PC_VARIANT_BITMAP_GROUP8 || v == PC_VARIANT_BITMAP_LANE);
+        const int cls = v == PC_VARIANT_MATRIX ? 2
+                         : (v == PC_VARIANT_BITMAP_WARP || v == PC_VARIANT_BITMAP_GROUP8 || v == PC_VARIANT_BITMAP_LANE)
+                               ? 1
+                               : 0;
         for (int r = 0; r < repeats; ++r) {
             std::vector<double> ms;
             uint64_t c = 0;
@@ -585,6 +607,7 @@ pc_status pc_selector_collect_insitu(pc_pgraph* pg, int32_t repeats, int32_t* ad
     }
     int32_t n_added = 0;
     std::lock_guard<std::mutex> lk(g_mu);
+    const int32_t gid = g_model.next_group++;
     for (size_t u = 0; u < U; ++u) {
         const float* f = &pg->part_features[u * kNumFeatures];
         if (!(f[1] > 0 && f[2] > 0)) continue;
@@ -597,6 +620,7 @@ pc_status pc_selector_collect_insitu(pc_pgraph* pg, int32_t repeats, int32_t* ad
         g_model.feats.insert(g_model.feats.end(), f, f + kNumFeatures);
         g_model.logms.insert(g_model.logms.end(), logms, logms + kMlpOut);
         g_model.mask.insert(g_model.mask.end(), msk, msk + kMlpOut);
+        g_model.group.push_back(gid);
         ++n_added;
     }
     if (added) *added = n_added;
@@ -626,6 +650,7 @@ pc_status pc_selector_add_samples(const float* feats, const float* log_ms, const
     g_model.feats.insert(g_model.feats.end(), feats, feats + (size_t)count * kNumFeatures);
     g_model.logms.insert(g_model.logms.end(), log_ms, log_ms + (size_t)count * kMlpOut);
     g_model.mask.insert(g_model.mask.end(), mask, mask + (size_t)count * kMlpOut);
+    g_model.group.insert(g_model.group.end(), (size_t)count, g_model.next_group++);
     return PC_OK;
 }
 
@@ -650,53 +675,147 @@ pc_status pc_selector_enable(int32_t on) {
     return PC_OK;
 }
 
-pc_status pc_selector_train(int32_t steps, float lr, uint64_t seed, float* final_loss) {
-    clear_error();
-    if (steps <= 0 || !(lr > 0.f)) return fail(PC_ERR_INVALID_INPUT, "bad argument");
-    if (pc_device_count() == 0) return fail(PC_ERR_NO_DEVICE, "no CUDA device is visible");
-    Model md;
-    {
-        std::lock_guard<std::mutex> lk(g_mu);
-        md.feats = g_model.feats;
-        md.logms = g_model.logms;
-        md.mask = g_model.mask;
-    }
-    const int n = (int)(md.feats.size() / kNumFeatures);
-    if (n < 2) return fail(PC_ERR_INVALID_INPUT, "collect at least two samples before training");
-    std::vector<float> X((size_t)n * kMlpIn);
-    for (int s = 0; s < n; ++s) features_to_inputs(&md.feats[(size_t)s * kNumFeatures], &X[(size_t)s * kMlpIn]);
-    for (int k = 0; k < kMlpIn; ++k) {
-        double m = 0, v = 0;
-        for (int s = 0; s < n; ++s) m += X[(size_t)s * kMlpIn + k];
-        m /= n;
-        for (int s = 0; s < n; ++s) v += (X[(size_t)s * kMlpIn + k] - m) * (X[(size_t)s * kMlpIn + k] - m);
-        v /= n;
-        md.mean[k] = (float)m;
-        md.stdv[k] = (float)std::max(1e-3, std::sqrt(v));
-        md.lo[k] = 1e30f;
-        md.hi[k] = -1e30f;
-        for (int s = 0; s < n; ++s) {
-            float& z = X[(size_t)s * kMlpIn + k];
-            z = (z - md.mean[k]) / md.stdv[k];
-            md.lo[k] = std::min(md.lo[k], z);
-            md.hi[k] = std::max(md.hi[k], z);
+}  // extern "C"
+
+namespace pc {
+
+// Fits a model to the samples idx of `data` (standardisation, He-uniform
+// initialisation from the counter-based generator, full-batch Adam on the GPU).
+static pc_status fit_model(const Model& data, const std::vector<size_t>& idx, int32_t steps, float lr, uint64_t seed,
+                           Model* md, float* loss) {
+    const int n = (int)idx.size();
+    std::vector<float> X((size_t)n * kMlpIn), Y((size_t)n * kMlpOut);
+    std::vector<uint8_t> M((size_t)n * kMlpOut);
+    for (int i = 0; i < n; ++i) {
+        const float* f = &data.feats[idx[i] * kNumFeatures];
+        features_to_inputs(f, &X[(size_t)i * kMlpIn]);
+        const float lw = log_work(f);
+        for (int o = 0; o < kMlpOut; ++o) {
+            Y[(size_t)i * kMlpOut + o] = data.logms[idx[i] * kMlpOut + o] - lw;
+            M[(size_t)i * kMlpOut + o] = data.mask[idx[i] * kMlpOut + o];
         }
     }
-    // He-uniform initialisation from the counter-based generator.
-    md.params.assign(kMlpParams, 0.f);
+    for (int k = 0; k < kMlpIn; ++k) {
+        double m = 0, v = 0;
+        for (int i = 0; i < n; ++i) m += X[(size_t)i * kMlpIn + k];
+        m /= n;
+        for (int i = 0; i < n; ++i) v += (X[(size_t)i * kMlpIn + k] - m) * (X[(size_t)i * kMlpIn + k] - m);
+        v /= n;
+        md->mean[k] = (float)m;
+        md->stdv[k] = (float)std::max(1e-3, std::sqrt(v));
+        md->lo[k] = 1e30f;
+        md->hi[k] = -1e30f;
+        for (int i = 0; i < n; ++i) {
+            float& z = X[(size_t)i * kMlpIn + k];
+            z = (z - md->mean[k]) / md->stdv[k];
+            md->lo[k] = std::min(md->lo[k], z);
+            md->hi[k] = std::max(md->hi[k], z);
+        }
+    }
+    md->params.assign(kMlpParams, 0.f);
     const uint64_t key = pc_graph_key(seed, 99);
     auto init = [&](int off, int fan_in, int count) {
         const double a = std::sqrt(6.0 / fan_in);
         for (int i = 0; i < count; ++i) {
             const double u = (double)(pc_draw(key, (uint64_t)(off + i)) >> 11) * (1.0 / 9007199254740992.0);
-            md.params[off + i] = (float)((2.0 * u - 1.0) * a);
+            md->params[off + i] = (float)((2.0 * u - 1.0) * a);
         }
     };
     init(kOffW1, kMlpIn, kMlpHidden * kMlpIn);
     init(kOffW2, kMlpHidden, kMlpHidden * kMlpHidden);
     init(kOffW3, kMlpHidden, kMlpOut * kMlpHidden);
+    return run_train_kernel(md->params, X, Y, M, n, steps, lr, loss, nullptr);
+}
+
+// Predicted log(ms) per variant for the samples idx of `data` under model md.
+static pc_status predict_samples(const Model& md, const Model& data, const std::vector<size_t>& idx,
+                                 std::vector<float>* out) {
+    const int n = (int)idx.size();
+    std::vector<float> X((size_t)n * kMlpIn);
+    for (int i = 0; i < n; ++i) standardise(md, &data.feats[idx[i] * kNumFeatures], &X[(size_t)i * kMlpIn]);
+    out->assign((size_t)n * kMlpOut, 0.f);
+    PC_TRY(run_forward(md.params, X.data(), n, out->data()));
+    for (int i = 0; i < n; ++i) {
+        const float lw = log_work(&data.feats[idx[i] * kNumFeatures]);
+        for (int o = 0; o < kMlpOut; ++o) (*out)[(size_t)i * kMlpOut + o] += lw;
+    }
+    return PC_OK;
+}
+
+}  // namespace pc
+
+extern "C" {
+
+pc_status pc_selector_train(int32_t steps, float lr, uint64_t seed, float* final_loss) {
+    clear_error();
+    if (steps <= 0 || !(lr > 0.f)) return fail(PC_ERR_INVALID_INPUT, "bad argument");
+    if (pc_device_count() == 0) return fail(PC_ERR_NO_DEVICE, "no CUDA device is visible");
+    Model data;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        data.feats = g_model.feats;
+        data.logms = g_model.logms;
+        data.mask = g_model.mask;
+        data.group = g_model.group;
+    }
+    const size_t n = data.feats.size() / kNumFeatures;
+    if (n < 2) return fail(PC_ERR_INVALID_INPUT, "collect at least two samples before training");
+    const HeuristicParams hp = heuristic_params();
+    // Judge margin by leave-one-group-out validation: for every collection
+    // group, a model fitted on the other groups plans the held-out units;
+    // the margin that gives the lowest measured total over all held-out
+    // units wins, +inf (keep the heuristic) when none beats the heuristic.
+    const float margins[] = {0.0f, 0.0487902f, 0.0953102f, 0.1823216f, 0.3364722f, INFINITY};
+    constexpr int kM = sizeof(margins) / sizeof(margins[0]);
+    double cost[kM] = {0};
+    std::vector<int32_t> gids(data.group.begin(), data.group.end());
+    std::sort(gids.begin(), gids.end());
+    gids.erase(std::unique(gids.begin(), gids.end()), gids.end());
+    bool validated = false;
+    if (gids.size() >= 2) {
+        for (int32_t g : gids) {
+            std::vector<size_t> tr, te;
+            for (size_t i = 0; i < n; ++i) (data.group[i] == g ? te : tr).push_back(i);
+            if (tr.size() < 2 || te.empty()) continue;
+            Model md;
+            PC_TRY(fit_model(data, tr, steps, lr, seed, &md, nullptr));
+            std::vector<float> Y;
+            PC_TRY(predict_samples(md, data, te, &Y));
+            for (size_t i = 0; i < te.size(); ++i) {
+                const size_t sidx = te[i];
+                const float* f = &data.feats[sidx * kNumFeatures];
+                const float* meas = &data.logms[sidx * kMlpOut];
+                const uint8_t* msk = &data.mask[sidx * kMlpOut];
+                const int h = tc::heuristic_choice(f, hp);
+                if (h < 0 || !msk[h]) continue;
+                float x[kMlpIn];
+                standardise(md, f, x);
+                bool inside = true;
+                for (int k = 0; k < kMlpIn; ++k) {
+                    const float span = md.hi[k] - md.lo[k];
+                    if (x[k] < md.lo[k] - 0.25f * span - 0.5f || x[k] > md.hi[k] + 0.25f * span + 0.5f) inside = false;
+                }
+                const float* y = &Y[i * kMlpOut];
+                int best = -1;
+                for (int v = 0; v < kMlpOut; ++v)
+                    if (tc::variant_feasible(v, f) && msk[v] && (best < 0 || y[v] < y[best])) best = v;
+                for (int k = 0; k < kM; ++k) {
+                    const int c = (inside && best >= 0 && y[h] - y[best] > margins[k]) ? best : h;
+                    cost[k] += std::exp((double)meas[c]);
+                }
+            }
+            validated = true;
+        }
+    }
+    int pick = validated ? kM - 1 : 1;  // unvalidated: the default 5 % margin
+    if (validated)
+        for (int k = kM - 2; k >= 0; --k)
+            if (cost[k] < cost[pick] * 0.999) pick = k;
+    std::vector<size_t> all(n);
+    for (size_t i = 0; i < n; ++i) all[i] = i;
+    Model md;
     float loss = 0.f;
-    PC_TRY(run_train_kernel(md.params, X, md.logms, md.mask, n, steps, lr, &loss, nullptr));
+    PC_TRY(fit_model(data, all, steps, lr, seed, &md, &loss));
     if (final_loss) *final_loss = loss;
     std::lock_guard<std::mutex> lk(g_mu);
     g_model.params = md.params;
@@ -704,8 +823,19 @@ pc_status pc_selector_train(int32_t steps, float lr, uint64_t seed, float* final
     memcpy(g_model.stdv, md.stdv, sizeof(md.stdv));
     memcpy(g_model.lo, md.lo, sizeof(md.lo));
     memcpy(g_model.hi, md.hi, sizeof(md.hi));
+    g_model.judge_log_margin = margins[pick];
+    g_model.heldout_gain = validated && cost[pick] > 0 ? cost[kM - 1] / cost[pick] : 0.0;
     g_model.trained = true;
     bump_version_locked();
+    return PC_OK;
+}
+
+pc_status pc_selector_judge(double* log_margin, double* heldout_gain) {
+    clear_error();
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_model.trained) return fail(PC_ERR_UNSUPPORTED, "the selector is not trained");
+    if (log_margin) *log_margin = g_model.judge_log_margin;
+    if (heldout_gain) *heldout_gain = g_model.heldout_gain;
     return PC_OK;
 }
 
@@ -722,7 +852,12 @@ pc_status pc_selector_predict(const float* feats, int32_t count, float* log_ms) 
     }
     std::vector<float> X((size_t)count * kMlpIn);
     for (int s = 0; s < count; ++s) standardise(md, feats + (size_t)s * kNumFeatures, &X[(size_t)s * kMlpIn]);
-    return run_forward(md.params, X.data(), count, log_ms);
+    PC_TRY(run_forward(md.params, X.data(), count, log_ms));
+    for (int s = 0; s < count; ++s) {
+        const float lw = log_work(feats + (size_t)s * kNumFeatures);
+        for (int o = 0; o < kMlpOut; ++o) log_ms[(size_t)s * kMlpOut + o] += lw;
+    }
+    return PC_OK;
 }
 
 pc_status pc_selector_get_heuristic(double* p) {
@@ -732,6 +867,7 @@ pc_status pc_selector_get_heuristic(double* p) {
     p[0] = hp.min_in_per_pivot_cta;
     p[1] = hp.warp_scan;
     p[2] = hp.group_scan;
+    p[3] = hp.matrix_scan;
     return PC_OK;
 }
 
@@ -742,11 +878,12 @@ pc_status pc_selector_set_heuristic(const double* p) {
     hp.min_in_per_pivot_cta = p[0];
     hp.warp_scan = p[1];
     hp.group_scan = p[2];
+    hp.matrix_scan = p[3];
     set_heuristic_params(hp);
     return PC_OK;
 }
 
-// Autotuner of the plain heuristic: grid search of its three thresholds that
+// Autotuner of the plain heuristic: grid search of its four thresholds that
 // minimises the summed measured time of its choices over the collected samples.
 pc_status pc_selector_autotune(double* tuned) {
     clear_error();
@@ -778,15 +915,18 @@ pc_status pc_selector_autotune(double* tuned) {
         for (double w : grid_scan)
             for (double g : grid_scan) {
                 if (g > w) continue;
-                HeuristicParams hp{a, w, g};
-                const double t = total(hp);
-                if (t < best_t) { best_t = t; best = hp; }
+                for (double mx : grid_scan) {
+                    HeuristicParams hp{a, w, g, mx};
+                    const double t = total(hp);
+                    if (t < best_t) { best_t = t; best = hp; }
+                }
             }
     set_heuristic_params(best);
     if (tuned) {
         tuned[0] = best.min_in_per_pivot_cta;
         tuned[1] = best.warp_scan;
         tuned[2] = best.group_scan;
+        tuned[3] = best.matrix_scan;
     }
     return PC_OK;
 }
@@ -798,7 +938,7 @@ pc_status pc_selector_save(const char* path) {
     if (!g_model.trained) return fail(PC_ERR_UNSUPPORTED, "the selector is not trained");
     FILE* f = fopen(path, "wb");
     if (!f) return fail(PC_ERR_INVALID_INPUT, std::string("cannot write ") + path);
-    const uint32_t magic = 0x50434D4Cu, np = kMlpParams;
+    const uint32_t magic = 0x50434D32u, np = kMlpParams;
     fwrite(&magic, 4, 1, f);
     fwrite(&np, 4, 1, f);
     fwrite(g_model.params.data(), 4, kMlpParams, f);
@@ -806,6 +946,7 @@ pc_status pc_selector_save(const char* path) {
     fwrite(g_model.stdv, 4, kMlpIn, f);
     fwrite(g_model.lo, 4, kMlpIn, f);
     fwrite(g_model.hi, 4, kMlpIn, f);
+    fwrite(&g_model.judge_log_margin, 4, 1, f);
     fclose(f);
     return PC_OK;
 }
@@ -818,10 +959,11 @@ pc_status pc_selector_load(const char* path) {
     uint32_t magic = 0, np = 0;
     Model md;
     md.params.resize(kMlpParams);
-    bool ok = fread(&magic, 4, 1, f) == 1 && fread(&np, 4, 1, f) == 1 && magic == 0x50434D4Cu && np == kMlpParams &&
+    bool ok = fread(&magic, 4, 1, f) == 1 && fread(&np, 4, 1, f) == 1 && magic == 0x50434D32u && np == kMlpParams &&
               fread(md.params.data(), 4, kMlpParams, f) == (size_t)kMlpParams &&
               fread(md.mean, 4, kMlpIn, f) == (size_t)kMlpIn && fread(md.stdv, 4, kMlpIn, f) == (size_t)kMlpIn &&
-              fread(md.lo, 4, kMlpIn, f) == (size_t)kMlpIn && fread(md.hi, 4, kMlpIn, f) == (size_t)kMlpIn;
+              fread(md.lo, 4, kMlpIn, f) == (size_t)kMlpIn && fread(md.hi, 4, kMlpIn, f) == (size_t)kMlpIn &&
+              fread(&md.judge_log_margin, 4, 1, f) == 1;
     fclose(f);
     if (!ok) return fail(PC_ERR_INVALID_INPUT, "not a selector model file");
     std::lock_guard<std::mutex> lk(g_mu);
@@ -830,6 +972,7 @@ pc_status pc_selector_load(const char* path) {
     memcpy(g_model.stdv, md.stdv, sizeof(md.stdv));
     memcpy(g_model.lo, md.lo, sizeof(md.lo));
     memcpy(g_model.hi, md.hi, sizeof(md.hi));
+    g_model.judge_log_margin = md.judge_log_margin;
     g_model.trained = true;
     bump_version_locked();
     return PC_OK;

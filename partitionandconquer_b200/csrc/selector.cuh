@@ -33,6 +33,7 @@ struct HeuristicParams {
     double min_in_per_pivot_cta = 32.0;  // in-edges per pivot to use a CTA-wide bitmap
     double warp_scan = 48.0;             // mean prefix bound for 32 lanes per in-neighbour
     double group_scan = 6.0;             // ... for 8 lanes per in-neighbour
+    double matrix_scan = 1e30;           // ... for the in-neighbour-major hub form (ids < 2^16)
 };
 HeuristicParams heuristic_params();
 void set_heuristic_params(const HeuristicParams& hp);

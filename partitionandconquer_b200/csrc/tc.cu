@@ -90,11 +90,21 @@ __global__ void k_unit_pivot_stats(const uint64_t* __restrict__ off, const uint3
 
 // In-edge statistics: a warp per vertex c streams its prefix N+(c); every
 // pivot b there has c as an in-neighbour and gains dplus[c] (the bound on
-// c's scan).  Lanes hitting the same unit are merged with __match_any_sync,
-// so one atomic per unit and 32 edges.
+// c's scan).  Lanes hitting the same unit are merged with __match_any_sync;
+// with kSmem (up to kScanStatsSmemUnits units) the per-unit sums gather in a
+// shared-memory histogram first, because almost every row starts with hub
+// ids and global atomics on the first units would serialise.
+constexpr uint32_t kScanStatsSmemUnits = 4096;
+
+template <bool kSmem>
 __global__ void k_unit_scan_stats(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
                                   const uint32_t* __restrict__ dplus, const int32_t* __restrict__ unit_of,
-                                  uint64_t n, unsigned long long* __restrict__ out) {
+                                  uint64_t n, uint32_t U, unsigned long long* __restrict__ out) {
+    extern __shared__ unsigned long long hist[];  // kSmem: 2 U counters (scan bound, long prefixes)
+    if (kSmem) {
+        for (uint32_t i = threadIdx.x; i < 2 * U; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+    }
     const int lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -109,9 +119,21 @@ __global__ void k_unit_scan_stats(const uint64_t* __restrict__ off, const int32_
             const unsigned peers = __match_any_sync(0xffffffffu, u);
             if (ok && lane == __ffs(peers) - 1) {
                 const unsigned long long cntp = (unsigned long long)__popc(peers);
-                atomicAdd(&out[(uint64_t)u * kRawStats + 5], cntp * dc);
-                if (dc >= 32) atomicAdd(&out[(uint64_t)u * kRawStats + 8], cntp);
+                if (kSmem) {
+                    atomicAdd(&hist[2 * u], cntp * dc);
+                    if (dc >= 32) atomicAdd(&hist[2 * u + 1], cntp);
+                } else {
+                    atomicAdd(&out[(uint64_t)u * kRawStats + 5], cntp * dc);
+                    if (dc >= 32) atomicAdd(&out[(uint64_t)u * kRawStats + 8], cntp);
+                }
             }
+        }
+    }
+    if (kSmem) {
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < U; i += blockDim.x) {
+            if (hist[2 * i]) atomicAdd(&out[(uint64_t)i * kRawStats + 5], hist[2 * i]);
+            if (hist[2 * i + 1]) atomicAdd(&out[(uint64_t)i * kRawStats + 8], hist[2 * i + 1]);
         }
     }
 }
@@ -163,9 +185,109 @@ __global__ void k_item_fill(const uint64_t* __restrict__ off, const uint32_t* __
     }
 }
 
+// H[b - lo][a >> 5] |= bit(a) for a in N+(b), one warp per pivot.
+__global__ void k_matrix_rows(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                              const uint32_t* __restrict__ dplus, int32_t lo, int32_t hi, uint32_t hwords,
+                              uint32_t* __restrict__ H) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t b = lo + warp; b < hi; b += nwarps) {
+        const int32_t* row = adj + off[b];
+        uint32_t* h = H + (uint64_t)(b - lo) * hwords;
+        for (uint32_t k = lane; k < dplus[b]; k += 32) {
+            const int32_t a = row[k];
+            atomicOr(&h[a >> 5], 1u << (a & 31));
+        }
+    }
+}
+
+// Warps take 32 in-neighbours c at a time from a global counter over
+// (lo, n); lanes locate S_c's pivot positions [k_lo, k_hi) by binary search
+// (N(c) is sorted, and min(hi, c) <= c keeps the search inside N+(c)).
+__global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t* __restrict__ off,
+                                                               const int32_t* __restrict__ adj,
+                                                               const uint32_t* __restrict__ dplus, int32_t lo,
+                                                               int32_t hi, uint64_t n, uint32_t hwords,
+                                                               const uint32_t* __restrict__ H,
+                                                               unsigned long long* __restrict__ next_c,
+                                                               unsigned long long* __restrict__ total,
+                                                               unsigned long long* __restrict__ unit_cost,
+                                                               int32_t unit) {
+    extern __shared__ uint32_t msm[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t* Sb = msm + (size_t)w * hwords;  // warp-private bitmap of S_c
+    for (uint32_t i = lane; i < hwords; i += 32) Sb[i] = 0;
+    __syncwarp();
+    unsigned long long cnt = 0;
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(next_c, 32ull);
+        base = __shfl_sync(0xffffffffu, base, 0) + (unsigned long long)lo + 1;
+        if (base >= n) break;
+        const long long t0 = unit_cost ? clock64() : 0;
+        const uint64_t c = base + lane;
+        uint64_t r = 0;
+        uint32_t klo = 0, khi = 0;
+        if (c < n) {
+            r = off[c];
+            const uint32_t dp = dplus[c];
+            const int32_t lim = (int64_t)c < (int64_t)hi ? (int32_t)c : hi;
+            khi = lower_bound_i32(adj + r, dp, lim);
+            klo = lower_bound_i32(adj + r, khi, lo);
+        }
+        unsigned todo = __ballot_sync(0xffffffffu, khi > klo);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int32_t* S = adj + __shfl_sync(0xffffffffu, r, src);
+            const uint32_t j0 = __shfl_sync(0xffffffffu, klo, src);
+            const uint32_t k = __shfl_sync(0xffffffffu, khi, src);
+            // word mode pays off where ceil(b/32) <= 2 j; build the bitmap
+            // of S_c only if some pivot of c will use it
+            const int32_t blast = S[k - 1];
+            const bool words = (uint32_t)((blast + 31) >> 5) <= 2 * (k - 1) || ((S[j0] + 31) >> 5) <= 2 * j0;
+            if (words) {
+                for (uint32_t i = lane; i < k; i += 32) {
+                    const int32_t a = S[i];
+                    atomicOr(&Sb[a >> 5], 1u << (a & 31));
+                }
+                __syncwarp();
+            }
+            for (uint32_t j = j0; j < k; ++j) {
+                const int32_t b = S[j];
+                const uint32_t* h = H + (uint64_t)(b - lo) * hwords;
+                const uint32_t nw = (uint32_t)(b + 31) >> 5;
+                if (words && nw <= 2 * j) {
+                    for (uint32_t x = lane; x < nw; x += 32) cnt += __popc(h[x] & Sb[x]);
+                } else {
+                    for (uint32_t i = lane; i < j; i += 32) {
+                        const int32_t a = S[i];
+                        cnt += (h[a >> 5] >> (a & 31)) & 1u;
+                    }
+                }
+            }
+            if (words) {
+                __syncwarp();
+                for (uint32_t i = lane; i < k; i += 32) Sb[S[i] >> 5] = 0;
+                __syncwarp();
+            }
+        }
+        if (unit_cost) {
+            __syncwarp();
+            if (lane == 0) atomicAdd(&unit_cost[unit], (unsigned long long)(clock64() - t0));
+        }
+    }
+    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0 && cnt) atomicAdd(total, cnt);
+}
+
 constexpr uint32_t kBitmapCapBits = 1u << 20;  // 128 KB of shared memory
 
 static bool bitmap_feasible(const float* f) { return f[4] <= (float)kBitmapCapBits; }
+// The in-neighbour-major form needs the unit's pivots to be the id range
+// [lo, hi) (contiguous partitions; tc_assign checks that) with hi <= 2^16.
+static bool matrix_feasible(const float* f) { return f[4] <= (float)kMatrixMaxId; }
 
 // Plain autotuned heuristic.  Thresholds come from heuristic_params(), which
 // the autotuner (pc_selector_autotune) may replace.
@@ -174,6 +296,7 @@ int heuristic_choice(const float* f, const HeuristicParams& hp) {
     if (ein <= 0 || sdp <= 0) return -1;
     const double scan = f[5] / std::max(1.0, ein);
     const double inpp = ein / std::max(1.0, npiv);
+    if (matrix_feasible(f) && inpp >= hp.min_in_per_pivot_cta && scan >= hp.matrix_scan) return PC_VARIANT_MATRIX;
     if (bitmap_feasible(f) && inpp >= hp.min_in_per_pivot_cta) {
         if (scan >= hp.warp_scan) return PC_VARIANT_BITMAP_WARP;
         if (scan >= hp.group_scan) return PC_VARIANT_BITMAP_GROUP8;
@@ -189,6 +312,7 @@ bool variant_feasible(int v, const float* f) {
         case PC_VARIANT_BITMAP_WARP:
         case PC_VARIANT_BITMAP_GROUP8:
         case PC_VARIANT_BITMAP_LANE: return bitmap_feasible(f);
+        case PC_VARIANT_MATRIX: return matrix_feasible(f);
         default: return v >= 0 && v < PC_NUM_VARIANTS;
     }
 }
@@ -292,7 +416,15 @@ static pc_status tc_features(pc_pgraph* pg) {
     PC_LAUNCHED();
     k_unit_pivot_stats<<<sms * 8, 256, 0, s>>>(pg->off, pg->dplus.as<uint32_t>(), unit_of, n, d_raw);
     PC_LAUNCHED();
-    k_unit_scan_stats<<<sms * 16, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), unit_of, n, d_raw);
+    if (U <= kScanStatsSmemUnits) {
+        const size_t smem = 2 * U * sizeof(unsigned long long);
+        PC_CUDA(cudaFuncSetAttribute(k_unit_scan_stats<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_unit_scan_stats<true><<<sms * 2, 1024, smem, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), unit_of, n,
+                                                           (uint32_t)U, d_raw);
+    } else {
+        k_unit_scan_stats<false><<<sms * 16, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), unit_of, n,
+                                                           (uint32_t)U, d_raw);
+    }
     PC_LAUNCHED();
     std::vector<unsigned long long> raw(U * kRawStats);
     PC_CUDA(cudaMemcpyAsync(raw.data(), d_raw, raw.size() * 8, cudaMemcpyDeviceToHost, s));
@@ -317,7 +449,38 @@ struct LaunchGroup {
     uint64_t npos = 0, item_bound = 0;
     double ein = 0;
     size_t units = 0;
+    std::vector<int32_t> unit_ids;  // matrix groups: one launch per unit (ranges not merged)
 };
+
+// Bytes of the resident pivot bitmap rows of a matrix unit [lo, hi).
+static uint64_t matrix_bytes(int64_t lo, int64_t hi) {
+    return (uint64_t)(hi - lo) * (uint64_t)((hi + 31) / 32) * 4;
+}
+
+// The in-neighbour-major form over one unit (ids [lo, hi)), all asynchronous:
+// rows H built from N+(b), then the walk over the in-neighbours.
+static pc_status run_matrix_unit(pc_pgraph* pg, int64_t lo, int64_t hi, int32_t unit, uint32_t* H,
+                                 unsigned long long* d_next, unsigned long long* d_total, unsigned long long* d_cost,
+                                 uint64_t* launches) {
+    cudaStream_t s = pg->g->stream;
+    const int sms = sm_count(pg->g->device);
+    const uint32_t hwords = (uint32_t)((hi + 31) / 32);
+    PC_CUDA(cudaMemsetAsync(H, 0, matrix_bytes(lo, hi), s));
+    PC_CUDA(cudaMemsetAsync(d_next, 0, 8, s));
+    k_matrix_rows<<<sms * 8, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), (int32_t)lo, (int32_t)hi, hwords,
+                                          H);
+    PC_LAUNCHED();
+    const size_t smem = (size_t)kMatrixWarps * hwords * 4;
+    PC_CUDA(cudaFuncSetAttribute(k_tc_matrix, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    PC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_matrix, kMatrixWarps * 32, smem));
+    k_tc_matrix<<<(unsigned)(sms * std::max(1, per_sm)), kMatrixWarps * 32, smem, s>>>(
+        pg->off, pg->adj, pg->dplus.as<uint32_t>(), (int32_t)lo, (int32_t)hi, pg->g->n, hwords, H, d_next, d_total,
+        d_cost, unit);
+    PC_LAUNCHED();
+    *launches += 2;
+    return PC_OK;
+}
 
 // Items never exceed min(pivots, in-edges) + in-edges / chunk; the float
 // in-edge feature is widened by 256 per unit for its rounding.
@@ -329,6 +492,17 @@ static void finish_group(LaunchGroup* gr) {
 // Launches one group (all asynchronous).
 static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long long* d_total, uint64_t* launches,
                            unsigned long long* d_cost) {
+    if (gr.v == PC_VARIANT_MATRIX) {
+        uint64_t hb = 0;
+        for (size_t i = 0; i < gr.unit_ids.size(); ++i) hb = std::max(hb, matrix_bytes(gr.ranges[2 * i], gr.ranges[2 * i + 1]));
+        uint32_t* H = pg->scratch.take<uint32_t>(hb / 4);
+        unsigned long long* d_next = pg->scratch.take<unsigned long long>(1);
+        if (!H || !d_next) return fail(PC_ERR_OOM, "scratch arena too small (internal sizing error)");
+        for (size_t i = 0; i < gr.unit_ids.size(); ++i)
+            PC_TRY(run_matrix_unit(pg, gr.ranges[2 * i], gr.ranges[2 * i + 1], gr.unit_ids[i], H, d_next, d_total,
+                                   d_cost, launches));
+        return PC_OK;
+    }
     const int32_t* unit_of = pg->unit_of.as<int32_t>();
     cudaStream_t s = pg->g->stream;
     const int v = gr.v;
@@ -422,8 +596,16 @@ static pc_status tc_execute(pc_pgraph* pg, const std::vector<int8_t>& assign, ui
         group_of[u] = v * kClasses + c;
         gr.v = v;
         gr.words = 1u << c;
-        if (!gr.ranges.empty() && gr.ranges.back() == lo[u]) gr.ranges.back() = hi[u];
-        else { gr.ranges.push_back(lo[u]); gr.ranges.push_back(hi[u]); }
+        if (v == PC_VARIANT_MATRIX) {
+            gr.ranges.push_back(lo[u]);
+            gr.ranges.push_back(hi[u]);
+            gr.unit_ids.push_back((int32_t)u);
+        } else if (!gr.ranges.empty() && gr.ranges.back() == lo[u]) {
+            gr.ranges.back() = hi[u];
+        } else {
+            gr.ranges.push_back(lo[u]);
+            gr.ranges.push_back(hi[u]);
+        }
         gr.npos += (uint64_t)(hi[u] - lo[u]);
         gr.ein += feat[u * kNumFeatures + 1];
         gr.units += 1;
@@ -431,6 +613,13 @@ static pc_status tc_execute(pc_pgraph* pg, const std::vector<int8_t>& assign, ui
     size_t need = 1024;
     for (LaunchGroup& gr : groups) {
         if (gr.ranges.empty()) continue;
+        if (gr.v == PC_VARIANT_MATRIX) {
+            uint64_t hb = 0;
+            for (size_t i = 0; i < gr.unit_ids.size(); ++i)
+                hb = std::max(hb, matrix_bytes(gr.ranges[2 * i], gr.ranges[2 * i + 1]));
+            need += hb + 2 * 256;
+            continue;
+        }
         finish_group(&gr);
         size_t tmpb = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, tmpb, (uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t)(gr.npos + 1),
@@ -515,12 +704,16 @@ pc_status tc_assign(pc_pgraph* pg, int32_t variant, const std::vector<float>& fe
     assign->assign(U, -1);
     if (variant >= 0) {
         if (variant >= PC_NUM_VARIANTS) return fail(PC_ERR_INVALID_INPUT, "unknown TC variant");
+        if (variant == PC_VARIANT_MATRIX && !pg->contiguous)
+            return fail(PC_ERR_UNSUPPORTED, "forced matrix variant: the partitions are not contiguous id ranges");
         for (size_t u = 0; u < U; ++u) {
             const float* f = &feat[u * kNumFeatures];
             if (f[1] <= 0 || f[2] <= 0) continue;
             if (!variant_feasible(variant, f))
-                return fail(PC_ERR_UNSUPPORTED,
-                            "forced bitmap variant: a pivot id exceeds the shared-memory bitmap capacity");
+                return fail(PC_ERR_UNSUPPORTED, variant == PC_VARIANT_MATRIX
+                                                    ? "forced matrix variant: a pivot id is 2^16 or above"
+                                                    : "forced bitmap variant: a pivot id exceeds the shared-memory "
+                                                      "bitmap capacity");
             (*assign)[u] = (int8_t)variant;
         }
         *selector_used = 0;
@@ -535,13 +728,16 @@ pc_status tc_assign(pc_pgraph* pg, int32_t variant, const std::vector<float>& fe
         *selector_used = learned ? 2 : 1;
         return PC_OK;
     }
-    const HeuristicParams hp = heuristic_params();
+    HeuristicParams hp = heuristic_params();
+    // the matrix form needs units that are id ranges
+    if (!pg->contiguous) hp.matrix_scan = INFINITY;
     if (learned) PC_TRY(selector_choose_batch(feat, U, assign));
     for (size_t u = 0; u < U; ++u) {
         const float* f = &feat[u * kNumFeatures];
         if (f[1] <= 0 || f[2] <= 0) { (*assign)[u] = -1; continue; }
         int v = learned ? (*assign)[u] : heuristic_choice(f, hp);
-        if (v < 0 || !variant_feasible(v, f)) v = heuristic_choice(f, hp);
+        if (v < 0 || !variant_feasible(v, f) || (v == PC_VARIANT_MATRIX && !pg->contiguous))
+            v = heuristic_choice(f, hp);
         (*assign)[u] = (int8_t)v;
     }
     pg->plan_key = key;
@@ -574,9 +770,10 @@ pc_status tc_profile_variant(pc_pgraph* pg, int variant, std::vector<double>* un
     PC_TRY(tc_ensure_features(pg));
     const size_t U = pg->unit_lo.size();
     std::vector<int8_t> assign(U, -1);
+    const bool ok = variant != PC_VARIANT_MATRIX || pg->contiguous;
     for (size_t u = 0; u < U; ++u) {
         const float* f = &pg->part_features[u * kNumFeatures];
-        if (f[1] > 0 && f[2] > 0 && variant_feasible(variant, f)) assign[u] = (int8_t)variant;
+        if (ok && f[1] > 0 && f[2] > 0 && variant_feasible(variant, f)) assign[u] = (int8_t)variant;
     }
     PC_TRY(tc_execute(pg, assign, count, nullptr, unit_ms));
     for (size_t u = 0; u < U; ++u)

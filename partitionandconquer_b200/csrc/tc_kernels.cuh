@@ -295,5 +295,32 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
     if (lane == 0 && cnt) atomicAdd(total, cnt);
 }
 
+
+// ---- in-neighbour-major form for hub units (variant "matrix") ----------------
+//
+// For a unit of pivots b in the id range [lo, hi) (hi <= kMatrixMaxId), the
+// pivot sets N+(b) are kept as bitmap rows H[b - lo] of hi bits in global
+// memory: (hi - lo) * hi / 8 bytes, 32 MB for the first 16 K ids, which stay
+// in L2.  The kernel then walks the in-neighbours c instead of the pivots:
+// S_c = N(c) & [0, min(hi, c)) is read once, and for every pivot b in
+// S_c & [lo, hi) at position j of S_c the count |S_c[0..j) & N+(b)| is taken
+// either by j bit probes into H[b] or by ceil(b/32) word-wise ANDs of H[b]
+// with a shared-memory bitmap of S_c and popcounts, whichever is cheaper.
+// Every (pivot, in-neighbour) pair of the unit is one pair (b, c) here, so the
+// count equals the pivot form's; what changes is that N(c) comes from DRAM
+// once per c instead of once per pivot.
+constexpr int kMatrixMaxId = 1 << 16;      // hi bound: rows of <= 8 KB, H <= 512 MB
+constexpr int kMatrixWarps = 8;            // warps per CTA
+constexpr int kMatrixWordsMax = kMatrixMaxId / 32;
+
+__device__ __forceinline__ uint32_t lower_bound_i32(const int32_t* __restrict__ p, uint32_t n, int32_t x) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (p[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
 }  // namespace tc
 }  // namespace pc

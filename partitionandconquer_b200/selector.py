@@ -56,6 +56,13 @@ def collect_insitu(pg, repeats: int = 2) -> int:
     return int(added.value)
 
 
+def judge():
+    """(log margin, held-out gain) of the trained selector's judge."""
+    m, g = C.c_double(), C.c_double()
+    check(lib.pc_selector_judge(C.byref(m), C.byref(g)))
+    return float(m.value), float(g.value)
+
+
 def num_samples() -> int:
     return int(lib.pc_selector_num_samples())
 
@@ -90,19 +97,21 @@ def predict(feats) -> np.ndarray:
 
 
 def autotune() -> np.ndarray:
-    out = np.empty(3, np.float64)
+    out = np.empty(4, np.float64)
     check(lib.pc_selector_autotune(ptr(out)))
     return out
 
 
 def get_heuristic() -> np.ndarray:
-    out = np.empty(3, np.float64)
+    out = np.empty(4, np.float64)
     check(lib.pc_selector_get_heuristic(ptr(out)))
     return out
 
 
 def set_heuristic(params):
     p = _lib.as_array(params, np.float64)
+    if p.size != 4:
+        raise ValueError("four thresholds: in-edges per pivot, 32-lane, 8-lane and matrix prefix lengths")
     check(lib.pc_selector_set_heuristic(ptr(p)))
 
 

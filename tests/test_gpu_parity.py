@@ -71,7 +71,16 @@ def test_triangle_count_all_variants(gpu, O, cases):
     for cid, vl, el, w, v2p, g in cases:
         t = O.tc_merge(vl, el)
         pg = _pg(pc, g, v2p)
+        contiguous = v2p is None or bool(np.all(np.diff(v2p) >= 0))
+        f = pc.selector.unit_features(pg)
+        work = (f[:, 1] > 0) & (f[:, 2] > 0)
+        # (a graph without edges runs no kernel, so nothing is refused)
+        matrix_ok = (contiguous and not bool(np.any(work & (f[:, 4] > 1 << 16)))) or el.size == 0
         for vname, v in list(pc.VARIANTS.items()) + [("heuristic", pc.VARIANT_HEURISTIC), ("auto", pc.VARIANT_AUTO)]:
+            if vname == "matrix" and not matrix_ok:
+                with pytest.raises(pc.PCError):  # needs units that are id ranges below 2^16
+                    pg.triangle_count(variant=v)
+                continue
             got = pg.triangle_count(variant=v)
             assert got == t, (cid, vname, got, t)
         assert pg.solve_triangle_counting_galloping() == 6 * t, cid
@@ -279,6 +288,43 @@ def test_config1_rmat16(gpu, O):
     assert int(lab.astype(np.int64).sum()) == s["cdlp_sum"]
     lcc = pg.solve_lcc_merge()
     assert int(np.isnan(lcc).sum()) == s["lcc_nan"]
+
+
+@pytest.mark.parametrize("scale,P", [(16, 4), (19, 16)])
+def test_matrix_form_on_hub_units(gpu, O, scale, P):
+    """The in-neighbour-major form (resident pivot bitmap rows, word-AND and
+    bit probes) on every unit whose ids are below 2^16, the other units by
+    the usual kernels: exact counts, forced where every unit qualifies."""
+    pc = gpu
+    sel = pc.selector
+    vl, el, _ = pc.HostCSR.rmat(scale, 16, 3).arrays()
+    n = vl.size - 1
+    t = O.tc_merge(vl, el)
+    g = pc.Graph(vlist=vl, elist=el)
+    pg = pc.Partitioned_Graph(g, pc.equal_vertex_partition(n, P))
+    saved = sel.get_heuristic()
+    try:
+        sel.set_heuristic([1.0, 48.0, 6.0, 0.0])  # matrix wherever it is feasible
+        c, st = pg.triangle_count(variant=pc.VARIANT_HEURISTIC, stats=True)
+        assert c == t and st.variant_hist[pc.VARIANTS["matrix"]] > 0
+        if n <= 1 << 16:
+            assert pg.triangle_count(variant=pc.VARIANTS["matrix"]) == t
+        else:
+            with pytest.raises(pc.PCError):
+                pg.triangle_count(variant=pc.VARIANTS["matrix"])
+    finally:
+        sel.set_heuristic(saved)
+    pg.close()
+    # non-contiguous partitions: the heuristic never picks the matrix form
+    pg = pc.Partitioned_Graph(g, np.random.default_rng(1).integers(0, P, n).astype(np.int32))
+    sel.set_heuristic([1.0, 48.0, 6.0, 0.0])
+    try:
+        c, st = pg.triangle_count(variant=pc.VARIANT_HEURISTIC, stats=True)
+        assert c == t and st.variant_hist[pc.VARIANTS["matrix"]] == 0
+    finally:
+        sel.set_heuristic(saved)
+    pg.close()
+    g.close()
 
 
 def test_bitmap_kernels_every_set_shape(gpu, O):

@@ -9,7 +9,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-IN, H, OUT = 12, 64, 6
+from partitionandconquer_b200._lib import MLP_HIDDEN as H, MLP_IN as IN, MLP_OUT as OUT  # noqa: E402
 
 
 def unpack(p):
@@ -109,14 +109,14 @@ def test_selector_end_to_end_exact(gpu, O, tmp_path):
         pgs.append((pg, O.tc_merge(vl, el)))
         assert sel.collect(pg, max_units=16, repeats=1) > 0
     f, y, m = sel.samples()
-    assert f.shape[1] == 10 and y.shape[1] == 6 and m.any(axis=1).all()
+    assert f.shape[1] == 10 and y.shape[1] == pc.NUM_VARIANTS and m.any(axis=1).all()
     loss = sel.train(steps=400, lr=3e-3, seed=5)
     assert np.isfinite(loss)
     assert sel.trained()
     pred = sel.predict(f)
     assert pred.shape == y.shape and np.isfinite(pred).all()
     tuned = sel.autotune()
-    assert tuned.shape == (3,)
+    assert tuned.shape == (4,)
     for pg, t in pgs:
         assert pg.triangle_count(variant=pc.VARIANT_AUTO) == t
         c, st = pg.triangle_count(variant=pc.VARIANT_AUTO, stats=True)
@@ -124,7 +124,7 @@ def test_selector_end_to_end_exact(gpu, O, tmp_path):
         c, st = pg.triangle_count(variant=pc.VARIANT_HEURISTIC, stats=True)
         assert c == t and st.selector == 1
         plan = sel.plan(pg, pc.VARIANT_AUTO)
-        assert plan.dtype == np.int8 and plan.max() < 6
+        assert plan.dtype == np.int8 and plan.max() < pc.NUM_VARIANTS
     path = str(tmp_path / "sel.bin")
     sel.save(path)
     before = sel.predict(f)
@@ -157,7 +157,7 @@ def test_insitu_collection_charges_every_unit(gpu, O):
     f, y, m = sel.samples()
     assert f.shape[0] == added and m.any(axis=1).all()
     # the warp variants (hash, merge, gallop) run on every unit with work
-    assert m[:, 3:].all()
+    assert m[:, 3:6].all()
     assert np.isfinite(y[m.astype(bool)]).all()
     # per-unit shares of the hash run add up to about one full hash-variant run
     total = float(np.exp(y[:, 3]).sum())
