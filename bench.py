@@ -64,6 +64,8 @@ def parse():
                     help="comma list of per-config suites: algos (RMAT-22, P=256, all nine algorithms with full-size "
                          "parity against the reference on the host cores), skew (ER and Chung-Lu, n=2^24, m=2^28, "
                          "P=512), rmat25 (RMAT-25, P=2048); one JSON line per measurement")
+    ap.add_argument("--heuristic", default="",
+                    help="profiling runs: the plain heuristic's four thresholds, comma-separated")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: plain heuristic plan only, no selector training, e2e or CPU leg")
     return ap.parse_args()
@@ -352,6 +354,8 @@ def run_ours(args, dist):
     algo_bytes, W, e_plus = tc_algorithmic_bytes(vl, el)
     v2p = pc.equal_vertex_partition(n, args.partitions)
     if args.profile:
+        if args.heuristic:
+            pc.selector.set_heuristic([float(x) for x in args.heuristic.split(",")])
         g = pc.Graph(vlist=vl, elist=el)
         pg = pc.Partitioned_Graph(g, v2p)
         stream = torch.cuda.ExternalStream(g.stream())

@@ -15,6 +15,7 @@
 #include <cmath>
 
 #include "pc_internal.cuh"
+#include "selector.cuh"
 
 namespace pc {
 namespace ix {
@@ -302,6 +303,18 @@ using namespace pc;
 
 extern "C" {
 
+// LCC from per-vertex triangle counts: sum over v in N(u) of |N(u) & N(v)|
+// counts every triangle at u twice, so the reference's numerator
+// (src/Graph.cpp:2230-2261, 814-840) is exactly 2 t(u); the same single
+// IEEE division follows, NaN at degree 1 as in the reference.
+__global__ void k_lcc_from_triangles(const uint64_t* __restrict__ off, const unsigned long long* __restrict__ tri,
+                                     uint64_t n, double* __restrict__ lcc) {
+    const uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (u >= n) return;
+    const uint64_t du = off[u + 1] - off[u];
+    lcc[u] = du < 1 ? 0.0 : (double)(2 * tri[u]) / (double)(du * (du - 1));
+}
+
 pc_status pc_lcc(pc_pgraph* pg, int32_t method, double* out) {
     clear_error();
     if (!pg || !out) return fail(PC_ERR_INVALID_INPUT, "null argument");
@@ -309,13 +322,18 @@ pc_status pc_lcc(pc_pgraph* pg, int32_t method, double* out) {
     PC_TRY(use_device(pg->g));
     const uint64_t n = pg->g->n;
     if (n == 0) return PC_OK;
-    uint32_t* ecnt = nullptr;
-    PC_TRY(edge_counts(pg, &ecnt, n * 8 * 2 + 512));
+    cudaStream_t s = pg->g->stream;
+    // per-vertex triangle counts with the triangle-count plan (its variants,
+    // the learned or heuristic choice per unit) in per-vertex mode
+    DevBuf tri;
+    PC_TRY(tri.alloc(n * 8, "triangles per vertex"));
+    PC_CUDA(cudaMemsetAsync(tri.p, 0, n * 8, s));
+    uint64_t T = 0;
+    PC_TRY(tc_vertex_triangles(pg, PC_VARIANT_AUTO, tri.as<unsigned long long>(), &T));
+    PC_TRY(scratch_reserve(pg, n * 16 + 1024));
     double* lcc = pg->scratch.take<double>(n);
     double* lcc_api = pg->scratch.take<double>(n);
-    cudaStream_t s = pg->g->stream;
-    k_finalize<<<sm_count(pg->g->device) * 16, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), ecnt, n,
-                                                             nullptr, lcc);
+    k_lcc_from_triangles<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(pg->off, tri.as<unsigned long long>(), n, lcc);
     PC_LAUNCHED();
     PC_TRY(gather_to_api_f64(pg, lcc, lcc_api));
     PC_CUDA(cudaMemcpyAsync(out, lcc_api, n * 8, cudaMemcpyDeviceToHost, s));

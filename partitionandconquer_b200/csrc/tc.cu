@@ -202,15 +202,70 @@ __global__ void k_matrix_rows(const uint64_t* __restrict__ off, const int32_t* _
     }
 }
 
-// Warps take 32 in-neighbours c at a time from a global counter over
-// (lo, n); lanes locate S_c's pivot positions [k_lo, k_hi) by binary search
-// (N(c) is sorted, and min(hi, c) <= c keeps the search inside N+(c)).
+// The pairs (b, c) of one in-neighbour c: S = N(c) & [0, min(hi, c)), pivots
+// at positions [j0, k).  Each pivot b = S[j] is taken by the whole warp:
+// j probes into row b (lanes read consecutive S[i], the probes hit one row)
+// or ceil(b/32) coalesced words of row b ANDed with the bitmap of S,
+// whichever is fewer.  The bitmap is built only when some pivot uses it.
+__device__ __forceinline__ unsigned long long matrix_pairs(const int32_t* __restrict__ S, uint32_t j0, uint32_t k,
+                                                           int32_t lo, uint32_t hwords,
+                                                           const uint32_t* __restrict__ H, uint32_t* Sb, int lane) {
+    unsigned long long cnt = 0;
+    bool want = false;
+    for (uint32_t j = j0 + lane; j < k; j += 32) want |= (uint32_t)((S[j] + 31) >> 5) <= j;
+    const bool words = __any_sync(0xffffffffu, want);
+    if (words) {
+        for (uint32_t i = lane; i < k; i += 32) {
+            const int32_t a = S[i];
+            atomicOr(&Sb[a >> 5], 1u << (a & 31));
+        }
+        __syncwarp();
+    }
+    for (uint32_t j = j0; j < k; ++j) {
+        const int32_t b = S[j];
+        const uint32_t* h = H + (uint64_t)(b - lo) * hwords;
+        const uint32_t nw = (uint32_t)(b + 31) >> 5;
+        if (words && nw <= j) {
+            for (uint32_t x = lane; x < nw; x += 32) cnt += __popc(h[x] & Sb[x]);
+        } else {
+            for (uint32_t i = lane; i < j; i += 32) {
+                const int32_t a = S[i];
+                cnt += (h[a >> 5] >> (a & 31)) & 1u;
+            }
+        }
+    }
+    if (words) {
+        __syncwarp();
+        for (uint32_t i = lane; i < k; i += 32) Sb[S[i] >> 5] = 0;
+        __syncwarp();
+    }
+    return cnt;
+}
+
+// Pivot positions [klo, khi) of in-neighbour c in its row (N(c) is sorted,
+// and min(hi, c) <= c keeps the search inside N+(c)).
+__device__ __forceinline__ void matrix_span(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                                            const uint32_t* __restrict__ dplus, int32_t lo, int32_t hi, uint64_t c,
+                                            uint64_t* r, uint32_t* klo, uint32_t* khi) {
+    *r = off[c];
+    const int32_t lim = (int64_t)c < (int64_t)hi ? (int32_t)c : hi;
+    *khi = lower_bound_i32(adj + *r, dplus[c], lim);
+    *klo = lower_bound_i32(adj + *r, *khi, lo);
+}
+
+// In-neighbours c run in two phases.  The first kMatrixHeavy ids after lo
+// (the hubs, with the longest S_c) are taken one per warp from counter
+// next[0]; the rest 32 at a time from next[1], lanes locating the 32 spans
+// at once.  One-at-a-time for the hubs keeps a single warp from holding a
+// batch of 32 hubs at the end of the launch.
+constexpr uint64_t kMatrixHeavy = 65536;
+
 __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t* __restrict__ off,
                                                                const int32_t* __restrict__ adj,
                                                                const uint32_t* __restrict__ dplus, int32_t lo,
                                                                int32_t hi, uint64_t n, uint32_t hwords,
                                                                const uint32_t* __restrict__ H,
-                                                               unsigned long long* __restrict__ next_c,
+                                                               unsigned long long* __restrict__ next,
                                                                unsigned long long* __restrict__ total,
                                                                unsigned long long* __restrict__ unit_cost,
                                                                int32_t unit) {
@@ -219,23 +274,31 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
     uint32_t* Sb = msm + (size_t)w * hwords;  // warp-private bitmap of S_c
     for (uint32_t i = lane; i < hwords; i += 32) Sb[i] = 0;
     __syncwarp();
+    const long long t0 = unit_cost ? clock64() : 0;
     unsigned long long cnt = 0;
-    for (;;) {
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(next_c, 32ull);
-        base = __shfl_sync(0xffffffffu, base, 0) + (unsigned long long)lo + 1;
+    const uint64_t c1 = (uint64_t)lo + 1 + kMatrixHeavy < n ? (uint64_t)lo + 1 + kMatrixHeavy : n;
+    for (;;) {  // phase 1: one hub in-neighbour per grab
+        unsigned long long q = 0;
+        if (lane == 0) q = atomicAdd(&next[0], 1ull);
+        const uint64_t c = __shfl_sync(0xffffffffu, q, 0) + (uint64_t)lo + 1;
+        if (c >= c1) break;
+        uint64_t r = 0;
+        uint32_t klo = 0, khi = 0;
+        if (lane == 0) matrix_span(off, adj, dplus, lo, hi, c, &r, &klo, &khi);
+        r = __shfl_sync(0xffffffffu, r, 0);
+        klo = __shfl_sync(0xffffffffu, klo, 0);
+        khi = __shfl_sync(0xffffffffu, khi, 0);
+        if (khi > klo) cnt += matrix_pairs(adj + r, klo, khi, lo, hwords, H, Sb, lane);
+    }
+    for (;;) {  // phase 2: 32 in-neighbours per grab
+        unsigned long long q = 0;
+        if (lane == 0) q = atomicAdd(&next[1], 32ull);
+        const uint64_t base = __shfl_sync(0xffffffffu, q, 0) + c1;
         if (base >= n) break;
-        const long long t0 = unit_cost ? clock64() : 0;
         const uint64_t c = base + lane;
         uint64_t r = 0;
         uint32_t klo = 0, khi = 0;
-        if (c < n) {
-            r = off[c];
-            const uint32_t dp = dplus[c];
-            const int32_t lim = (int64_t)c < (int64_t)hi ? (int32_t)c : hi;
-            khi = lower_bound_i32(adj + r, dp, lim);
-            klo = lower_bound_i32(adj + r, khi, lo);
-        }
+        if (c < n) matrix_span(off, adj, dplus, lo, hi, c, &r, &klo, &khi);
         unsigned todo = __ballot_sync(0xffffffffu, khi > klo);
         while (todo) {
             const int src = __ffs(todo) - 1;
@@ -243,40 +306,12 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
             const int32_t* S = adj + __shfl_sync(0xffffffffu, r, src);
             const uint32_t j0 = __shfl_sync(0xffffffffu, klo, src);
             const uint32_t k = __shfl_sync(0xffffffffu, khi, src);
-            // word mode pays off where ceil(b/32) <= 2 j; build the bitmap
-            // of S_c only if some pivot of c will use it
-            const int32_t blast = S[k - 1];
-            const bool words = (uint32_t)((blast + 31) >> 5) <= 2 * (k - 1) || ((S[j0] + 31) >> 5) <= 2 * j0;
-            if (words) {
-                for (uint32_t i = lane; i < k; i += 32) {
-                    const int32_t a = S[i];
-                    atomicOr(&Sb[a >> 5], 1u << (a & 31));
-                }
-                __syncwarp();
-            }
-            for (uint32_t j = j0; j < k; ++j) {
-                const int32_t b = S[j];
-                const uint32_t* h = H + (uint64_t)(b - lo) * hwords;
-                const uint32_t nw = (uint32_t)(b + 31) >> 5;
-                if (words && nw <= 2 * j) {
-                    for (uint32_t x = lane; x < nw; x += 32) cnt += __popc(h[x] & Sb[x]);
-                } else {
-                    for (uint32_t i = lane; i < j; i += 32) {
-                        const int32_t a = S[i];
-                        cnt += (h[a >> 5] >> (a & 31)) & 1u;
-                    }
-                }
-            }
-            if (words) {
-                __syncwarp();
-                for (uint32_t i = lane; i < k; i += 32) Sb[S[i] >> 5] = 0;
-                __syncwarp();
-            }
+            cnt += matrix_pairs(S, j0, k, lo, hwords, H, Sb, lane);
         }
-        if (unit_cost) {
-            __syncwarp();
-            if (lane == 0) atomicAdd(&unit_cost[unit], (unsigned long long)(clock64() - t0));
-        }
+    }
+    if (unit_cost) {
+        __syncwarp();
+        if (lane == 0) atomicAdd(&unit_cost[unit], (unsigned long long)(clock64() - t0));
     }
     for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if (lane == 0 && cnt) atomicAdd(total, cnt);
@@ -351,40 +386,52 @@ static BitmapShape bitmap_shape(uint32_t max_pivot_plus1) {
     return sh;
 }
 
-template <int K, int G>
-static pc_status launch_bitmap_kg(unsigned grid, size_t smem, cudaStream_t s, const uint64_t* off, const int32_t* adj,
-                                  const uint32_t* dp, const int32_t* plist, const Item* items, const uint32_t* nitems,
-                                  uint32_t* next, unsigned long long* total, uint32_t words, unsigned long long* cost,
-                                  const int32_t* unit_of) {
-    PC_CUDA(cudaFuncSetAttribute(k_tc_bitmap<K, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_tc_bitmap<K, G><<<grid, kCtaThreads, smem, s>>>(off, adj, dp, plist, items, nitems, next, total, words, cost,
-                                                      unit_of);
+// Arguments of one bitmap-kernel launch.
+struct BitmapLaunch {
+    unsigned grid;
+    size_t smem;
+    cudaStream_t s;
+    const uint64_t* off;
+    const int32_t* adj;
+    const uint32_t* dp;
+    const int32_t* plist;
+    const Item* items;
+    const uint32_t* nitems;
+    uint32_t* next;
+    unsigned long long* total;
+    uint32_t words;
+    unsigned long long* cost;
+    const int32_t* unit_of;
+    unsigned long long* tri;  // per-vertex triangle counts (LCC), or null
+};
+
+template <int K, int G, bool kVC>
+static pc_status launch_bitmap_kgv(const BitmapLaunch& L) {
+    PC_CUDA(cudaFuncSetAttribute(k_tc_bitmap<K, G, kVC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+    k_tc_bitmap<K, G, kVC><<<L.grid, kCtaThreads, L.smem, L.s>>>(L.off, L.adj, L.dp, L.plist, L.items, L.nitems, L.next,
+                                                               L.total, L.words, L.cost, L.unit_of, L.tri);
     return PC_OK;
 }
 
 template <int K>
-static pc_status launch_bitmap_k(int G, unsigned grid, size_t smem, cudaStream_t s, const uint64_t* off,
-                                 const int32_t* adj, const uint32_t* dp, const int32_t* plist, const Item* items,
-                                 const uint32_t* nitems, uint32_t* next, unsigned long long* total, uint32_t words,
-                                 unsigned long long* cost, const int32_t* uo) {
-    if (G == 32)
-        return launch_bitmap_kg<K, 32>(grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
-    if (G == 8)
-        return launch_bitmap_kg<K, 8>(grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
-    return launch_bitmap_kg<K, 1>(grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
+static pc_status launch_bitmap_k(int G, const BitmapLaunch& L) {
+    if (L.tri) {
+        if (G == 32) return launch_bitmap_kgv<K, 32, true>(L);
+        if (G == 8) return launch_bitmap_kgv<K, 8, true>(L);
+        return launch_bitmap_kgv<K, 1, true>(L);
+    }
+    if (G == 32) return launch_bitmap_kgv<K, 32, false>(L);
+    if (G == 8) return launch_bitmap_kgv<K, 8, false>(L);
+    return launch_bitmap_kgv<K, 1, false>(L);
 }
 
-static pc_status launch_bitmap(int K, int G, unsigned grid, size_t smem, cudaStream_t s, const uint64_t* off,
-                               const int32_t* adj, const uint32_t* dp, const int32_t* plist, const Item* items,
-                               const uint32_t* nitems, uint32_t* next, unsigned long long* total, uint32_t words,
-                               unsigned long long* cost, const int32_t* uo) {
+static pc_status launch_bitmap(int K, int G, const BitmapLaunch& L) {
     switch (K) {
-        case 1: return launch_bitmap_k<1>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
-        case 2: return launch_bitmap_k<2>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
-        case 4: return launch_bitmap_k<4>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
-        case 8: return launch_bitmap_k<8>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
-        default:
-            return launch_bitmap_k<16>(G, grid, smem, s, off, adj, dp, plist, items, nitems, next, total, words, cost, uo);
+        case 1: return launch_bitmap_k<1>(G, L);
+        case 2: return launch_bitmap_k<2>(G, L);
+        case 4: return launch_bitmap_k<4>(G, L);
+        case 8: return launch_bitmap_k<8>(G, L);
+        default: return launch_bitmap_k<16>(G, L);
     }
 }
 
@@ -466,7 +513,7 @@ static pc_status run_matrix_unit(pc_pgraph* pg, int64_t lo, int64_t hi, int32_t 
     const int sms = sm_count(pg->g->device);
     const uint32_t hwords = (uint32_t)((hi + 31) / 32);
     PC_CUDA(cudaMemsetAsync(H, 0, matrix_bytes(lo, hi), s));
-    PC_CUDA(cudaMemsetAsync(d_next, 0, 8, s));
+    PC_CUDA(cudaMemsetAsync(d_next, 0, 16, s));
     k_matrix_rows<<<sms * 8, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), (int32_t)lo, (int32_t)hi, hwords,
                                           H);
     PC_LAUNCHED();
@@ -491,12 +538,12 @@ static void finish_group(LaunchGroup* gr) {
 
 // Launches one group (all asynchronous).
 static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long long* d_total, uint64_t* launches,
-                           unsigned long long* d_cost) {
+                           unsigned long long* d_cost, unsigned long long* d_tri) {
     if (gr.v == PC_VARIANT_MATRIX) {
         uint64_t hb = 0;
         for (size_t i = 0; i < gr.unit_ids.size(); ++i) hb = std::max(hb, matrix_bytes(gr.ranges[2 * i], gr.ranges[2 * i + 1]));
         uint32_t* H = pg->scratch.take<uint32_t>(hb / 4);
-        unsigned long long* d_next = pg->scratch.take<unsigned long long>(1);
+        unsigned long long* d_next = pg->scratch.take<unsigned long long>(2);
         if (!H || !d_next) return fail(PC_ERR_OOM, "scratch arena too small (internal sizing error)");
         for (size_t i = 0; i < gr.unit_ids.size(); ++i)
             PC_TRY(run_matrix_unit(pg, gr.ranges[2 * i], gr.ranges[2 * i + 1], gr.unit_ids[i], H, d_next, d_total,
@@ -542,23 +589,50 @@ static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long l
     *launches += 3;
     const uint32_t* d_nitems = d_next + 1;
     if (is_bitmap(v)) {
-        const unsigned grid =
-            (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms * sh.ctas_per_sm, gr.item_bound));
+        BitmapLaunch L;
+        L.smem = sh.smem + (d_tri ? (size_t)kHubHist * 4 : 0);
+        const int cps = d_tri ? (int)std::max<size_t>(1, std::min<size_t>(4, (220 * 1024) / (L.smem + 1024)))
+                              : sh.ctas_per_sm;
+        L.grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms * cps, gr.item_bound));
+        L.s = s;
+        L.off = pg->off;
+        L.adj = pg->adj;
+        L.dp = dp;
+        L.plist = plist;
+        L.items = d_items;
+        L.nitems = d_nitems;
+        L.next = d_next;
+        L.total = d_total;
+        L.words = sh.words;
+        L.cost = d_cost;
+        L.unit_of = unit_of;
+        L.tri = d_tri;
         const int Gsel = v == PC_VARIANT_BITMAP_WARP ? 32 : (v == PC_VARIANT_BITMAP_GROUP8 ? 8 : 1);
-        PC_TRY(launch_bitmap(sh.K, Gsel, grid, sh.smem, s, pg->off, pg->adj, dp, plist, d_items, d_nitems, d_next,
-                             d_total, sh.words, d_cost, unit_of));
+        PC_TRY(launch_bitmap(sh.K, Gsel, L));
     } else {
         const unsigned grid = (unsigned)std::max<uint64_t>(
             1, std::min<uint64_t>((uint64_t)sms * 8, ceil_div(gr.item_bound, kWarpCtaWarps)));
-        if (v == PC_VARIANT_HASH_WARP)
-            k_tc_warp<kModeHash><<<grid, kWarpCtaWarps * 32, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems,
-                                                                     d_next, d_total, d_cost, unit_of);
-        else if (v == PC_VARIANT_MERGE_LANE)
-            k_tc_warp<kModeMerge><<<grid, kWarpCtaWarps * 32, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems,
-                                                                      d_next, d_total, d_cost, unit_of);
-        else
-            k_tc_warp<kModeGallop><<<grid, kWarpCtaWarps * 32, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems,
-                                                                       d_next, d_total, d_cost, unit_of);
+        const unsigned bs = kWarpCtaWarps * 32;
+        if (d_tri) {
+            if (v == PC_VARIANT_HASH_WARP)
+                k_tc_warp<kModeHash, true><<<grid, bs, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems, d_next,
+                                                               d_total, d_cost, unit_of, d_tri);
+            else if (v == PC_VARIANT_MERGE_LANE)
+                k_tc_warp<kModeMerge, true><<<grid, bs, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems, d_next,
+                                                                d_total, d_cost, unit_of, d_tri);
+            else
+                k_tc_warp<kModeGallop, true><<<grid, bs, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems,
+                                                                 d_next, d_total, d_cost, unit_of, d_tri);
+        } else if (v == PC_VARIANT_HASH_WARP) {
+            k_tc_warp<kModeHash><<<grid, bs, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems, d_next, d_total,
+                                                     d_cost, unit_of);
+        } else if (v == PC_VARIANT_MERGE_LANE) {
+            k_tc_warp<kModeMerge><<<grid, bs, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems, d_next, d_total,
+                                                      d_cost, unit_of);
+        } else {
+            k_tc_warp<kModeGallop><<<grid, bs, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems, d_next, d_total,
+                                                       d_cost, unit_of);
+        }
     }
     PC_LAUNCHED();
     *launches += 1;
@@ -572,7 +646,7 @@ static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long l
 // unit gets its group's time in proportion to its cycles: the unit's cost
 // inside a full run, where it shares the GPU with the other units.
 static pc_status tc_execute(pc_pgraph* pg, const std::vector<int8_t>& assign, uint64_t* count, pc_tc_stats* stats,
-                            std::vector<double>* unit_ms = nullptr) {
+                            std::vector<double>* unit_ms = nullptr, unsigned long long* d_tri = nullptr) {
     cudaStream_t s = pg->g->stream;
     const std::vector<int64_t>& lo = pg->unit_lo;
     const std::vector<int64_t>& hi = pg->unit_hi;
@@ -651,7 +725,7 @@ static pc_status tc_execute(pc_pgraph* pg, const std::vector<int8_t>& assign, ui
         const LaunchGroup& gr = groups[gi];
         if (gr.ranges.empty()) continue;
         if (unit_ms) PC_CUDA(cudaEventRecord(gev[2 * gi], s));
-        PC_TRY(run_group(pg, gr, d_total, &launches, d_cost));
+        PC_TRY(run_group(pg, gr, d_total, &launches, d_cost, d_tri));
         if (unit_ms) PC_CUDA(cudaEventRecord(gev[2 * gi + 1], s));
     }
     PC_CUDA(cudaEventRecord(pg->ev1, s));
@@ -760,6 +834,26 @@ pc_status tc_count(pc_pgraph* pg, int32_t variant, uint64_t* count, pc_tc_stats*
     PC_TRY(tc_execute(pg, assign, count, stats));
     if (stats) stats->selector = sel;
     return PC_OK;
+}
+
+// Per-vertex triangle counts (each triangle adds 1 to each of its three
+// vertices) into d_tri (n zeroed counters, outside the scratch arena) under
+// the plan of `variant`; the matrix form has no per-vertex mode, so its units
+// run with the 32-lane bitmap kernel.  Returns the triangle count.
+pc_status tc_vertex_triangles(pc_pgraph* pg, int32_t variant, unsigned long long* d_tri, uint64_t* count) {
+    PC_TRY(tc_ensure_features(pg));
+    const size_t U = pg->unit_lo.size();
+    *count = 0;
+    if (U == 0 || pg->g->m == 0) return PC_OK;
+    std::vector<int8_t> assign;
+    int sel = 0;
+    PC_TRY(tc_assign(pg, variant, pg->part_features, U, &assign, &sel));
+    for (size_t u = 0; u < U; ++u) {
+        if (assign[u] != PC_VARIANT_MATRIX) continue;
+        const float* f = &pg->part_features[u * kNumFeatures];
+        assign[u] = (int8_t)(bitmap_feasible(f) ? PC_VARIANT_BITMAP_WARP : PC_VARIANT_HASH_WARP);
+    }
+    return tc_execute(pg, assign, count, nullptr, nullptr, d_tri);
 }
 
 // Runs one variant on every unit it can take (all units with work; bitmap

@@ -33,6 +33,7 @@ constexpr int kCtaThreads = 512;    // threads per CTA of the bitmap kernels
 constexpr int kHashSlots = 512;     // slots per warp-private hash table
 constexpr int kHashCap = 256;       // max pivot set size for the hash kernel
 constexpr int kWarpCtaWarps = 8;    // warps per CTA of the warp kernels
+constexpr int kHubHist = 8192;      // per-vertex counting: ids below this count in shared memory
 
 enum WarpMode { kModeHash = 0, kModeMerge = 1, kModeGallop = 2 };
 
@@ -75,17 +76,31 @@ __device__ __forceinline__ void group_barrier(int id, int nthreads) {
 // Pipelined group-of-G prefix scan: the load of the next G ids is issued
 // before the current ones are tested, so two loads per lane are in flight.
 // Stops at the first id >= b and never reads past lim = dplus[c].
-template <int G>
+// Per-vertex triangle counts (kVC): every triangle found adds 1 to its
+// lowest vertex a; ids below kHubHist go to a shared-memory histogram
+// (almost every hit is a hub), the rest to the global counts.
+__device__ __forceinline__ void count_vertex(int32_t a, unsigned long long* __restrict__ tri, uint32_t* hist) {
+    if (a < kHubHist) atomicAdd(&hist[a], 1u);
+    else atomicAdd(&tri[a], 1ull);
+}
+
+template <int G, bool kVC = false>
 __device__ __forceinline__ uint32_t scan_prefix_pipelined(const int32_t* __restrict__ row, uint32_t lim, int32_t b,
                                                           int gl, unsigned gmask,
-                                                          const uint32_t* __restrict__ bm) {
+                                                          const uint32_t* __restrict__ bm,
+                                                          unsigned long long* __restrict__ tri = nullptr,
+                                                          uint32_t* hist = nullptr) {
     uint32_t hits = 0;
     uint32_t i = gl;
     int32_t a = i < lim ? __ldg(row + i) : 0x7fffffff;
     for (;;) {
         const uint32_t inext = i + G;
         const int32_t an = inext < lim ? __ldg(row + inext) : 0x7fffffff;
-        if (a < b) hits += (bm[a >> 5] >> (a & 31)) & 1u;
+        if (a < b) {
+            const uint32_t bit = (bm[a >> 5] >> (a & 31)) & 1u;
+            hits += bit;
+            if (kVC && bit) count_vertex(a, tri, hist);
+        }
         int32_t last;
         if constexpr (G == 1) last = a;
         else last = __shfl_sync(gmask, a, G - 1, G);
@@ -103,7 +118,7 @@ __device__ __forceinline__ uint32_t scan_prefix_pipelined(const int32_t* __restr
 // (id, row offset, prefix length) is fetched 32 at a time with one coalesced
 // load and 32 independent gathers, then handed to groups of G lanes by
 // shuffles; each group scans one prefix with scan_prefix_pipelined.
-template <int K, int G>
+template <int K, int G, bool kVC = false>
 __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __restrict__ off,
                                                            const int32_t* __restrict__ adj,
                                                            const uint32_t* __restrict__ dplus,
@@ -114,7 +129,8 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
                                                            unsigned long long* __restrict__ total,
                                                            uint32_t bm_words,
                                                            unsigned long long* __restrict__ unit_cost,
-                                                           const int32_t* __restrict__ unit_of) {
+                                                           const int32_t* __restrict__ unit_of,
+                                                           unsigned long long* __restrict__ tri = nullptr) {
     extern __shared__ uint32_t smem[];
     __shared__ uint32_t s_item[16];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -122,7 +138,9 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
     const int nsets = (kCtaThreads / 32) / K;
     const int set_threads = K * 32, tis = wi * 32 + lane;
     uint32_t* bm = smem + (size_t)set * bm_words;
-    for (uint32_t i = tid; i < (uint32_t)nsets * bm_words; i += blockDim.x) smem[i] = 0;
+    uint32_t* hist = smem + (size_t)nsets * bm_words;  // kVC: kHubHist counters after the sets
+    const uint32_t zero_words = (uint32_t)nsets * bm_words + (kVC ? (uint32_t)kHubHist : 0u);
+    for (uint32_t i = tid; i < zero_words; i += blockDim.x) smem[i] = 0;
     __syncthreads();
     auto set_sync = [&]() {
         if constexpr (K == 1) __syncwarp();
@@ -150,6 +168,7 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
         set_sync();
         const uint64_t in0 = rb + dp + (uint64_t)I.j0;
         const uint64_t in1 = min(rb + dp + (uint64_t)I.j1, re);
+        unsigned long long hb = 0;  // kVC: this item's triangles at pivot b
         for (uint64_t base = in0 + (uint64_t)wi * 32; base < in1; base += (uint64_t)set_threads) {
             const uint64_t e = base + lane;
             const bool ok = e < in1;
@@ -165,8 +184,22 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
                 const uint64_t rcj = __shfl_sync(0xffffffffu, rc, src);
                 uint32_t limj = __shfl_sync(0xffffffffu, lim, src);
                 if (j >= nb) limj = 0;
-                if (limj) cnt += scan_prefix_pipelined<G>(adj + rcj, limj, b, gl, gmask, bm);
+                if (kVC) {
+                    const int32_t cj = __shfl_sync(0xffffffffu, c, src);
+                    if (limj) {
+                        const uint32_t h = scan_prefix_pipelined<G, true>(adj + rcj, limj, b, gl, gmask, bm, tri, hist);
+                        cnt += h;
+                        hb += h;
+                        if (h) atomicAdd(&tri[cj], (unsigned long long)h);
+                    }
+                } else if (limj) {
+                    cnt += scan_prefix_pipelined<G>(adj + rcj, limj, b, gl, gmask, bm);
+                }
             }
+        }
+        if (kVC) {
+            for (int o = 16; o; o >>= 1) hb += __shfl_xor_sync(0xffffffffu, hb, o);
+            if (lane == 0 && hb) atomicAdd(&tri[b], hb);
         }
         set_sync();
         for (uint32_t k = tis; k < dp; k += set_threads) bm[adj[rb + k] >> 5] = 0;
@@ -176,6 +209,11 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
     }
     for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if (lane == 0 && cnt) atomicAdd(total, cnt);
+    if (kVC) {
+        __syncthreads();
+        for (uint32_t i = tid; i < (uint32_t)kHubHist; i += blockDim.x)
+            if (hist[i]) atomicAdd(&tri[i], (unsigned long long)hist[i]);
+    }
 }
 
 __device__ __forceinline__ uint32_t hash_slot(int32_t a) { return ((uint32_t)a * 0x9E3779B1u) >> (32 - 9); }
@@ -215,9 +253,51 @@ __device__ __forceinline__ uint32_t gallop_below(const int32_t* __restrict__ x, 
     return c;
 }
 
+// merge_below / gallop_below with per-vertex counting of every match (kVC).
+template <bool kVC>
+__device__ __forceinline__ uint32_t merge_below_vc(const int32_t* __restrict__ x, uint32_t nx,
+                                                   const int32_t* __restrict__ y, uint32_t ny, int32_t thr,
+                                                   unsigned long long* __restrict__ tri, uint32_t* hist) {
+    uint32_t i = 0, j = 0, c = 0;
+    while (i < nx && j < ny) {
+        const int32_t a = x[i], bb = y[j];
+        if (a >= thr || bb >= thr) break;
+        if (a < bb) ++i;
+        else if (a > bb) ++j;
+        else {
+            ++c;
+            if (kVC) count_vertex(a, tri, hist);
+            ++i;
+            ++j;
+        }
+    }
+    return c;
+}
+
+template <bool kVC>
+__device__ __forceinline__ uint32_t gallop_below_vc(const int32_t* __restrict__ x, uint32_t nx,
+                                                    const int32_t* __restrict__ y, uint32_t ny, int32_t thr,
+                                                    unsigned long long* __restrict__ tri, uint32_t* hist) {
+    uint32_t c = 0;
+    for (uint32_t i = 0; i < nx; ++i) {
+        const int32_t a = x[i];
+        if (a >= thr) break;
+        uint32_t lo = 0, hi = ny;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (y[mid] < a) lo = mid + 1; else hi = mid;
+        }
+        if (lo < ny && y[lo] == a) {
+            ++c;
+            if (kVC) count_vertex(a, tri, hist);
+        }
+    }
+    return c;
+}
+
 // Warp kernels: one item (pivot, <= kChunkWarp in-neighbours) per warp, one
 // lane per in-neighbour.
-template <int MODE>
+template <int MODE, bool kVC = false>
 __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* __restrict__ off,
                                                                 const int32_t* __restrict__ adj,
                                                                 const uint32_t* __restrict__ dplus,
@@ -227,10 +307,16 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
                                                                 uint32_t* __restrict__ next_item,
                                                                 unsigned long long* __restrict__ total,
                                                                 unsigned long long* __restrict__ unit_cost,
-                                                                const int32_t* __restrict__ unit_of) {
+                                                                const int32_t* __restrict__ unit_of,
+                                                                unsigned long long* __restrict__ tri = nullptr) {
     __shared__ int32_t table[MODE == kModeHash ? kWarpCtaWarps : 1][MODE == kModeHash ? kHashSlots : 1];
+    __shared__ uint32_t hist[kVC ? kHubHist : 1];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int32_t* T = table[MODE == kModeHash ? w : 0];
+    if (kVC) {
+        for (int i = threadIdx.x; i < kHubHist; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+    }
     if (MODE == kModeHash) {
         for (int s = lane; s < kHashSlots; s += 32) T[s] = -1;
         __syncwarp();
@@ -243,6 +329,7 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= nitems) break;
         const long long t0 = unit_cost ? clock64() : 0;
+        const unsigned long long cnt_item0 = cnt;
         const Item I = items[it];
         const int32_t b = pivot_at(plist, I.pos);
         const uint64_t rb = off[b], re = off[b + 1];
@@ -261,16 +348,23 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
                 const int32_t c = adj[e];
                 const int32_t* row = adj + off[c];
                 const uint32_t lim = dplus[c];
+                uint32_t h = 0;
                 for (uint32_t i = 0; i < lim; ++i) {
                     const int32_t a = __ldg(row + i);
                     if (a >= b) break;
                     uint32_t s = hash_slot(a);
                     int32_t key;
                     while ((key = T[s]) != -1) {
-                        if (key == a) { ++cnt; break; }
+                        if (key == a) {
+                            ++h;
+                            if (kVC) count_vertex(a, tri, hist);
+                            break;
+                        }
                         s = (s + 1) & (kHashSlots - 1);
                     }
                 }
+                cnt += h;
+                if (kVC && h) atomicAdd(&tri[c], (unsigned long long)h);
             }
             __syncwarp();
             for (int s = lane; s < kHashSlots; s += 32) T[s] = -1;
@@ -278,21 +372,36 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
         } else if (MODE == kModeGallop) {
             for (uint64_t e = in0 + lane; e < in1; e += 32) {
                 const int32_t c = adj[e];
-                cnt += gallop_below(adj + off[c], dplus[c], nb, dp, b);
+                const uint32_t h = gallop_below_vc<kVC>(adj + off[c], dplus[c], nb, dp, b, tri, hist);
+                cnt += h;
+                if (kVC && h) atomicAdd(&tri[c], (unsigned long long)h);
             }
         } else {
             for (uint64_t e = in0 + lane; e < in1; e += 32) {
                 const int32_t c = adj[e];
-                cnt += merge_below(adj + off[c], dplus[c], nb, dp, b);
+                const uint32_t h = merge_below_vc<kVC>(adj + off[c], dplus[c], nb, dp, b, tri, hist);
+                cnt += h;
+                if (kVC && h) atomicAdd(&tri[c], (unsigned long long)h);
             }
         }
         if (unit_cost) {
             __syncwarp();
             if (lane == 0) atomicAdd(&unit_cost[unit_of[b]], (unsigned long long)(clock64() - t0));
         }
+        if (kVC) {
+            // this item's triangles at pivot b: the warp's hits since the item began
+            unsigned long long hb = cnt - cnt_item0;
+            for (int o = 16; o; o >>= 1) hb += __shfl_xor_sync(0xffffffffu, hb, o);
+            if (lane == 0 && hb) atomicAdd(&tri[b], hb);
+        }
     }
     for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if (lane == 0 && cnt) atomicAdd(total, cnt);
+    if (kVC) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < kHubHist; i += blockDim.x)
+            if (hist[i]) atomicAdd(&tri[i], (unsigned long long)hist[i]);
+    }
 }
 
 
