@@ -1,14 +1,13 @@
-// Per-edge common-neighbour counts (LCC, all-edge Jaccard), Jaccard over a
-// query list, and batched pair / k-set intersection counts (sm_100a).
+// LCC and all-edge Jaccard on top of the triangle-count kernels, Jaccard
+// over a query list, and batched pair / k-set intersection counts (sm_100a).
 //
-// Per-edge counts c({u,v}) = |N(u) & N(v)| are built by listing every
-// triangle once in the pivot form of the TC kernels (a < b < c found at pivot
-// b from in-neighbour c) and adding 1 to its three edges.  An undirected edge
-// {x, y}, y < x, is counted at its oriented slot: position k of y in row x
-// (k < dplus[x]).  A finalisation pass reads, for every CSR entry, its own
-// slot or its twin's, and forms the Jaccard ratio and the LCC numerator
-// sum_{v in N(u)} c({u,v}) exactly as the reference defines them
-// (src/Graph.cpp:798-840).
+// Per-edge counts c({u,v}) = |N(u) & N(v)| come from the triangle-count
+// kernels in per-edge mode (tc_edge_triangles): every triangle adds 1 to its
+// three edges.  An undirected edge {x, y}, y < x, is counted at its oriented
+// slot: position k of y in row x (k < dplus[x]).  A finalisation pass reads,
+// for every CSR entry, its own slot or its twin's and forms the Jaccard ratio
+// exactly as the reference defines it (src/Graph.cpp:798-812).  LCC needs only
+// per-vertex triangle counts (tc_vertex_triangles).
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
@@ -20,18 +19,6 @@
 namespace pc {
 namespace ix {
 
-constexpr int kThreads = 512;
-constexpr int kChunk = 2048;     // in-neighbours per work item
-constexpr int kMapSlots = 4096;  // pivot map: open addressing
-constexpr int kMapCap = 2048;    // pivots with a larger set take the global path
-
-struct Item {
-    int32_t b;
-    int32_t j0;
-};
-
-__device__ __forceinline__ uint32_t map_slot(int32_t a) { return ((uint32_t)a * 0x9E3779B1u) >> (32 - 12); }
-
 // lower_bound of x in sorted p[0..n)
 __device__ __forceinline__ uint32_t lb(const int32_t* __restrict__ p, uint32_t n, int32_t x) {
     uint32_t lo = 0, hi = n;
@@ -40,110 +27,6 @@ __device__ __forceinline__ uint32_t lb(const int32_t* __restrict__ p, uint32_t n
         if (p[mid] < x) lo = mid + 1; else hi = mid;
     }
     return lo;
-}
-
-__global__ void k_items_count(const uint64_t* __restrict__ off, const uint32_t* __restrict__ dplus, uint64_t n,
-                              uint32_t* __restrict__ cnt) {
-    const uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (b > n) return;
-    if (b == n) { cnt[b] = 0; return; }
-    const uint32_t dp = dplus[b];
-    const uint64_t din = off[b + 1] - off[b] - dp;
-    cnt[b] = (dp == 0 || din == 0) ? 0u : (uint32_t)((din + kChunk - 1) / kChunk);
-}
-
-__global__ void k_items_fill(const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ start, uint64_t n,
-                             Item* __restrict__ items) {
-    const uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (b >= n) return;
-    const uint32_t c = cnt[b], s = start[b];
-    for (uint32_t j = 0; j < c; ++j) items[s + j] = Item{(int32_t)b, (int32_t)(j * kChunk)};
-}
-
-// Triangle listing with per-edge increments (one CTA per work item; warps
-// scan in-neighbour prefixes 32 ids at a time).
-__global__ void __launch_bounds__(kThreads) k_edge_counts(const uint64_t* __restrict__ off,
-                                                          const int32_t* __restrict__ adj,
-                                                          const uint32_t* __restrict__ dplus,
-                                                          const Item* __restrict__ items,
-                                                          const uint32_t* __restrict__ nitems_p,
-                                                          uint32_t* __restrict__ next_item,
-                                                          uint32_t* __restrict__ ecnt) {
-    extern __shared__ int32_t smap[];  // key | idx | hit, kMapSlots each
-    int32_t* key = smap;
-    uint32_t* idx = reinterpret_cast<uint32_t*>(smap + kMapSlots);
-    uint32_t* hit = reinterpret_cast<uint32_t*>(smap + 2 * kMapSlots);
-    __shared__ uint32_t s_item;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    for (int i = tid; i < kMapSlots; i += blockDim.x) { key[i] = -1; hit[i] = 0; }
-    const uint32_t nitems = *nitems_p;
-    for (;;) {
-        __syncthreads();
-        if (tid == 0) s_item = atomicAdd(next_item, 1u);
-        __syncthreads();
-        const uint32_t it = s_item;
-        if (it >= nitems) break;
-        const Item I = items[it];
-        const int32_t b = I.b;
-        const uint64_t rb = off[b], re = off[b + 1];
-        const uint32_t dp = dplus[b];
-        const bool use_map = dp <= (uint32_t)kMapCap;
-        if (use_map) {
-            for (uint32_t k = tid; k < dp; k += blockDim.x) {
-                const int32_t a = adj[rb + k];
-                uint32_t s = map_slot(a);
-                while (atomicCAS(&key[s], -1, a) != -1) s = (s + 1) & (kMapSlots - 1);
-                idx[s] = k;
-            }
-        }
-        __syncthreads();
-        const uint64_t in0 = rb + dp + (uint64_t)I.j0;
-        const uint64_t in1 = min(in0 + (uint64_t)kChunk, re);
-        for (uint64_t e = in0 + warp; e < in1; e += nw) {
-            const int32_t c = adj[e];
-            const uint64_t rc = off[c];
-            const uint32_t lim = dplus[c];
-            uint32_t pair_hits = 0, kb = 0xffffffffu;
-            for (uint32_t i0 = 0; i0 < lim; i0 += 32) {
-                const uint32_t i = i0 + lane;
-                const int32_t a = i < lim ? __ldg(adj + rc + i) : 0x7fffffff;
-                if (a < b) {
-                    bool found = false;
-                    if (use_map) {
-                        uint32_t s = map_slot(a);
-                        int32_t kk;
-                        while ((kk = key[s]) != -1) {
-                            if (kk == a) { found = true; atomicAdd(&hit[s], 1u); break; }
-                            s = (s + 1) & (kMapSlots - 1);
-                        }
-                    } else {
-                        const uint32_t p = lb(adj + rb, dp, a);
-                        if (p < dp && adj[rb + p] == a) { found = true; atomicAdd(&ecnt[rb + p], 1u); }
-                    }
-                    if (found) {
-                        ++pair_hits;
-                        atomicAdd(&ecnt[rc + i], 1u);  // edge {c, a}
-                    }
-                }
-                const unsigned at_b = __ballot_sync(0xffffffffu, a == b);
-                if (at_b) kb = i0 + __ffs(at_b) - 1;
-                const int32_t last = __shfl_sync(0xffffffffu, a, 31);
-                if (last >= b) break;
-            }
-            for (int o = 16; o; o >>= 1) pair_hits += __shfl_xor_sync(0xffffffffu, pair_hits, o);
-            if (lane == 0 && pair_hits && kb != 0xffffffffu) atomicAdd(&ecnt[rc + kb], pair_hits);  // edge {c, b}
-        }
-        __syncthreads();
-        if (use_map) {
-            for (int s = tid; s < kMapSlots; s += blockDim.x) {
-                if (key[s] != -1) {
-                    if (hit[s]) atomicAdd(&ecnt[rb + idx[s]], hit[s]);  // edges {b, a}
-                    key[s] = -1;
-                    hit[s] = 0;
-                }
-            }
-        }
-    }
 }
 
 // Count of the undirected edge behind CSR entry (u, v) at position e.
@@ -263,40 +146,6 @@ __global__ void k_make_pairs(const int32_t* __restrict__ q, int32_t nq, int32_t*
 
 using namespace ix;
 
-// Per-edge counts into a scratch array; returns it.
-static pc_status edge_counts(pc_pgraph* pg, uint32_t** ecnt_out, size_t extra_bytes) {
-    PC_TRY(ensure_dplus(pg));
-    const uint64_t n = pg->g->n, m = pg->g->m;
-    cudaStream_t s = pg->g->stream;
-    size_t tmpb = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, tmpb, (uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t)(n + 1), s);
-    const uint64_t item_bound = n + m / kChunk + 2;
-    PC_TRY(scratch_reserve(pg, m * 4 + (n + 1) * 8 + tmpb + item_bound * sizeof(Item) + 64 + extra_bytes));
-    uint32_t* ecnt = pg->scratch.take<uint32_t>(std::max<uint64_t>(m, 1));
-    uint32_t* cnt = pg->scratch.take<uint32_t>(n + 1);
-    uint32_t* start = pg->scratch.take<uint32_t>(n + 1);
-    void* tmp = pg->scratch.take<char>(tmpb);
-    Item* items = pg->scratch.take<Item>(item_bound);
-    uint32_t* next = pg->scratch.take<uint32_t>(1);
-    if (!ecnt || !cnt || !start || !tmp || !items || !next) return fail(PC_ERR_OOM, "scratch sizing error");
-    PC_CUDA(cudaMemsetAsync(ecnt, 0, std::max<uint64_t>(m, 1) * 4, s));
-    PC_CUDA(cudaMemsetAsync(next, 0, 4, s));
-    const uint32_t* dp = pg->dplus.as<uint32_t>();
-    k_items_count<<<(unsigned)ceil_div(n + 1, 256), 256, 0, s>>>(pg->off, dp, n, cnt);
-    PC_LAUNCHED();
-    PC_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmpb, cnt, start, (int64_t)(n + 1), s));
-    count_launch();
-    k_items_fill<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(cnt, start, n, items);
-    PC_LAUNCHED();
-    const int sms = sm_count(pg->g->device);
-    const int smem = kMapSlots * 12;
-    PC_CUDA(cudaFuncSetAttribute(k_edge_counts, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    k_edge_counts<<<sms * 2, kThreads, smem, s>>>(pg->off, pg->adj, dp, items, start + n, next, ecnt);
-    PC_LAUNCHED();
-    *ecnt_out = ecnt;
-    return PC_OK;
-}
-
 }  // namespace pc
 
 using namespace pc;
@@ -346,12 +195,18 @@ pc_status pc_jaccard_edges(pc_pgraph* pg, float* out) {
     PC_TRY(use_device(pg->g));
     const uint64_t n = pg->g->n, m = pg->g->m;
     if (m == 0) return PC_OK;
-    uint32_t* ecnt = nullptr;
-    PC_TRY(edge_counts(pg, &ecnt, m * 4 + 512));
-    float* jac = pg->scratch.take<float>(m);
     cudaStream_t s = pg->g->stream;
-    k_finalize<<<sm_count(pg->g->device) * 16, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), ecnt, n,
-                                                             jac, nullptr);
+    // per-edge triangle counts with the triangle-count plan (its variants,
+    // the learned or heuristic choice per unit) in per-edge mode
+    DevBuf ecnt;
+    PC_TRY(ecnt.alloc(m * 4, "triangles per edge"));
+    PC_CUDA(cudaMemsetAsync(ecnt.p, 0, m * 4, s));
+    uint64_t T = 0;
+    PC_TRY(tc_edge_triangles(pg, PC_VARIANT_AUTO, ecnt.as<uint32_t>(), &T));
+    PC_TRY(scratch_reserve(pg, m * 4 + 1024));
+    float* jac = pg->scratch.take<float>(m);
+    k_finalize<<<sm_count(pg->g->device) * 16, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(),
+                                                             ecnt.as<uint32_t>(), n, jac, nullptr);
     PC_LAUNCHED();
     // entries are in the graph's own CSR order (internal ids are the graph's ids)
     PC_CUDA(cudaMemcpyAsync(out, jac, m * 4, cudaMemcpyDeviceToHost, s));

@@ -56,6 +56,7 @@ pc_status tc_count(pc_pgraph* pg, int32_t variant, uint64_t* count, pc_tc_stats*
 pc_status tc_time_unit(pc_pgraph* pg, size_t unit, int variant, double* ms, uint64_t* count);
 pc_status tc_profile_variant(pc_pgraph* pg, int variant, std::vector<double>* unit_ms, uint64_t* count);
 pc_status tc_vertex_triangles(pc_pgraph* pg, int32_t variant, unsigned long long* d_tri, uint64_t* count);
+pc_status tc_edge_triangles(pc_pgraph* pg, int32_t variant, uint32_t* d_ecnt, uint64_t* count);
 pc_status tc_assign(pc_pgraph* pg, int32_t variant, const std::vector<float>& feat, size_t U,
                     std::vector<int8_t>* assign, int* selector_used);
 pc_status tc_ensure_features(pc_pgraph* pg);

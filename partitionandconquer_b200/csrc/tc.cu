@@ -403,26 +403,31 @@ struct BitmapLaunch {
     unsigned long long* cost;
     const int32_t* unit_of;
     unsigned long long* tri;  // per-vertex triangle counts (LCC), or null
+    uint32_t* ecnt;           // per-edge counts at the oriented slots (Jaccard), or null
 };
 
-template <int K, int G, bool kVC>
+template <int K, int G, bool kVC, bool kEC>
 static pc_status launch_bitmap_kgv(const BitmapLaunch& L) {
-    PC_CUDA(cudaFuncSetAttribute(k_tc_bitmap<K, G, kVC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
-    k_tc_bitmap<K, G, kVC><<<L.grid, kCtaThreads, L.smem, L.s>>>(L.off, L.adj, L.dp, L.plist, L.items, L.nitems, L.next,
-                                                               L.total, L.words, L.cost, L.unit_of, L.tri);
+    PC_CUDA(cudaFuncSetAttribute(k_tc_bitmap<K, G, kVC, kEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)L.smem));
+    k_tc_bitmap<K, G, kVC, kEC><<<L.grid, kCtaThreads, L.smem, L.s>>>(L.off, L.adj, L.dp, L.plist, L.items, L.nitems,
+                                                                    L.next, L.total, L.words, L.cost, L.unit_of,
+                                                                    L.tri, L.ecnt);
     return PC_OK;
+}
+
+template <int K, bool kVC, bool kEC>
+static pc_status launch_bitmap_kmode(int G, const BitmapLaunch& L) {
+    if (G == 32) return launch_bitmap_kgv<K, 32, kVC, kEC>(L);
+    if (G == 8) return launch_bitmap_kgv<K, 8, kVC, kEC>(L);
+    return launch_bitmap_kgv<K, 1, kVC, kEC>(L);
 }
 
 template <int K>
 static pc_status launch_bitmap_k(int G, const BitmapLaunch& L) {
-    if (L.tri) {
-        if (G == 32) return launch_bitmap_kgv<K, 32, true>(L);
-        if (G == 8) return launch_bitmap_kgv<K, 8, true>(L);
-        return launch_bitmap_kgv<K, 1, true>(L);
-    }
-    if (G == 32) return launch_bitmap_kgv<K, 32, false>(L);
-    if (G == 8) return launch_bitmap_kgv<K, 8, false>(L);
-    return launch_bitmap_kgv<K, 1, false>(L);
+    if (L.tri) return launch_bitmap_kmode<K, true, false>(G, L);
+    if (L.ecnt) return launch_bitmap_kmode<K, false, true>(G, L);
+    return launch_bitmap_kmode<K, false, false>(G, L);
 }
 
 static pc_status launch_bitmap(int K, int G, const BitmapLaunch& L) {
@@ -538,7 +543,7 @@ static void finish_group(LaunchGroup* gr) {
 
 // Launches one group (all asynchronous).
 static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long long* d_total, uint64_t* launches,
-                           unsigned long long* d_cost, unsigned long long* d_tri) {
+                           unsigned long long* d_cost, unsigned long long* d_tri, uint32_t* d_ecnt) {
     if (gr.v == PC_VARIANT_MATRIX) {
         uint64_t hb = 0;
         for (size_t i = 0; i < gr.unit_ids.size(); ++i) hb = std::max(hb, matrix_bytes(gr.ranges[2 * i], gr.ranges[2 * i + 1]));
@@ -590,9 +595,11 @@ static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long l
     const uint32_t* d_nitems = d_next + 1;
     if (is_bitmap(v)) {
         BitmapLaunch L;
-        L.smem = sh.smem + (d_tri ? (size_t)kHubHist * 4 : 0);
-        const int cps = d_tri ? (int)std::max<size_t>(1, std::min<size_t>(4, (220 * 1024) / (L.smem + 1024)))
-                              : sh.ctas_per_sm;
+        const size_t nsets = (size_t)(kCtaThreads / 32 / sh.K);
+        L.smem = sh.smem + (d_tri ? (size_t)kHubHist * 4 : 0) + (d_ecnt ? nsets * ((sh.words + 7) / 8) * 4 : 0);
+        const int cps = (d_tri || d_ecnt)
+                            ? (int)std::max<size_t>(1, std::min<size_t>(4, (220 * 1024) / (L.smem + 1024)))
+                            : sh.ctas_per_sm;
         L.grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms * cps, gr.item_bound));
         L.s = s;
         L.off = pg->off;
@@ -607,13 +614,26 @@ static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long l
         L.cost = d_cost;
         L.unit_of = unit_of;
         L.tri = d_tri;
+        L.ecnt = d_ecnt;
         const int Gsel = v == PC_VARIANT_BITMAP_WARP ? 32 : (v == PC_VARIANT_BITMAP_GROUP8 ? 8 : 1);
         PC_TRY(launch_bitmap(sh.K, Gsel, L));
     } else {
         const unsigned grid = (unsigned)std::max<uint64_t>(
             1, std::min<uint64_t>((uint64_t)sms * 8, ceil_div(gr.item_bound, kWarpCtaWarps)));
         const unsigned bs = kWarpCtaWarps * 32;
-        if (d_tri) {
+        if (d_ecnt) {
+            if (v == PC_VARIANT_HASH_WARP)
+                k_tc_warp<kModeHash, false, true><<<grid, bs, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems,
+                                                                      d_next, d_total, d_cost, unit_of, nullptr, d_ecnt);
+            else if (v == PC_VARIANT_MERGE_LANE)
+                k_tc_warp<kModeMerge, false, true><<<grid, bs, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems,
+                                                                       d_next, d_total, d_cost, unit_of, nullptr,
+                                                                       d_ecnt);
+            else
+                k_tc_warp<kModeGallop, false, true><<<grid, bs, 0, s>>>(pg->off, pg->adj, dp, plist, d_items,
+                                                                        d_nitems, d_next, d_total, d_cost, unit_of,
+                                                                        nullptr, d_ecnt);
+        } else if (d_tri) {
             if (v == PC_VARIANT_HASH_WARP)
                 k_tc_warp<kModeHash, true><<<grid, bs, 0, s>>>(pg->off, pg->adj, dp, plist, d_items, d_nitems, d_next,
                                                                d_total, d_cost, unit_of, d_tri);
@@ -646,7 +666,8 @@ static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long l
 // unit gets its group's time in proportion to its cycles: the unit's cost
 // inside a full run, where it shares the GPU with the other units.
 static pc_status tc_execute(pc_pgraph* pg, const std::vector<int8_t>& assign, uint64_t* count, pc_tc_stats* stats,
-                            std::vector<double>* unit_ms = nullptr, unsigned long long* d_tri = nullptr) {
+                            std::vector<double>* unit_ms = nullptr, unsigned long long* d_tri = nullptr,
+                            uint32_t* d_ecnt = nullptr) {
     cudaStream_t s = pg->g->stream;
     const std::vector<int64_t>& lo = pg->unit_lo;
     const std::vector<int64_t>& hi = pg->unit_hi;
@@ -725,7 +746,7 @@ static pc_status tc_execute(pc_pgraph* pg, const std::vector<int8_t>& assign, ui
         const LaunchGroup& gr = groups[gi];
         if (gr.ranges.empty()) continue;
         if (unit_ms) PC_CUDA(cudaEventRecord(gev[2 * gi], s));
-        PC_TRY(run_group(pg, gr, d_total, &launches, d_cost, d_tri));
+        PC_TRY(run_group(pg, gr, d_total, &launches, d_cost, d_tri, d_ecnt));
         if (unit_ms) PC_CUDA(cudaEventRecord(gev[2 * gi + 1], s));
     }
     PC_CUDA(cudaEventRecord(pg->ev1, s));
@@ -854,6 +875,26 @@ pc_status tc_vertex_triangles(pc_pgraph* pg, int32_t variant, unsigned long long
         assign[u] = (int8_t)(bitmap_feasible(f) ? PC_VARIANT_BITMAP_WARP : PC_VARIANT_HASH_WARP);
     }
     return tc_execute(pg, assign, count, nullptr, nullptr, d_tri);
+}
+
+// Per-edge triangle counts at the oriented slots (the slot of edge {x, y},
+// y < x, is the position of y in row x) into d_ecnt (m zeroed counters,
+// outside the scratch arena), under the plan of `variant`; matrix units run
+// with the 32-lane bitmap kernel.  Returns the triangle count.
+pc_status tc_edge_triangles(pc_pgraph* pg, int32_t variant, uint32_t* d_ecnt, uint64_t* count) {
+    PC_TRY(tc_ensure_features(pg));
+    const size_t U = pg->unit_lo.size();
+    *count = 0;
+    if (U == 0 || pg->g->m == 0) return PC_OK;
+    std::vector<int8_t> assign;
+    int sel = 0;
+    PC_TRY(tc_assign(pg, variant, pg->part_features, U, &assign, &sel));
+    for (size_t u = 0; u < U; ++u) {
+        if (assign[u] != PC_VARIANT_MATRIX) continue;
+        const float* f = &pg->part_features[u * kNumFeatures];
+        assign[u] = (int8_t)(bitmap_feasible(f) ? PC_VARIANT_BITMAP_WARP : PC_VARIANT_HASH_WARP);
+    }
+    return tc_execute(pg, assign, count, nullptr, nullptr, nullptr, d_ecnt);
 }
 
 // Runs one variant on every unit it can take (all units with work; bitmap

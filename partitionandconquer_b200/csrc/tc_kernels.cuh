@@ -84,14 +84,33 @@ __device__ __forceinline__ void count_vertex(int32_t a, unsigned long long* __re
     else atomicAdd(&tri[a], 1ull);
 }
 
-template <int G, bool kVC = false>
+// Position of a in the pivot set: bits of the bitmap below a, from the
+// superblock prefix sb (one count per 8 words) and at most 8 word popcounts.
+__device__ __forceinline__ uint32_t rank_in_set(const uint32_t* __restrict__ bm, const uint32_t* __restrict__ sb,
+                                                int32_t a) {
+    const uint32_t w = (uint32_t)a >> 5;
+    uint32_t r = sb[w >> 3];
+    for (uint32_t x = w & ~7u; x < w; ++x) r += __popc(bm[x]);
+    return r + __popc(bm[w] & ((1u << (a & 31)) - 1u));
+}
+
+// Modes of the pivot-form kernels: count only; kVC per-vertex triangle
+// counts (LCC); kEC per-edge counts at the oriented slots (Jaccard): every
+// triangle a < b < c adds 1 to the slot of a in row c (its scan index), to
+// the slot of a in row b (its rank in the pivot set) and, once per pair,
+// its hits to the slot of b in row c (where the scan stops).
+template <int G, bool kVC = false, bool kEC = false>
 __device__ __forceinline__ uint32_t scan_prefix_pipelined(const int32_t* __restrict__ row, uint32_t lim, int32_t b,
                                                           int gl, unsigned gmask,
                                                           const uint32_t* __restrict__ bm,
                                                           unsigned long long* __restrict__ tri = nullptr,
-                                                          uint32_t* hist = nullptr) {
+                                                          uint32_t* hist = nullptr,
+                                                          uint32_t* __restrict__ ec_c = nullptr,
+                                                          uint32_t* __restrict__ ec_b = nullptr,
+                                                          const uint32_t* __restrict__ sb = nullptr) {
     uint32_t hits = 0;
     uint32_t i = gl;
+    int32_t kb = -1;  // kEC: index of b in the row, seen by one lane of the group
     int32_t a = i < lim ? __ldg(row + i) : 0x7fffffff;
     for (;;) {
         const uint32_t inext = i + G;
@@ -100,6 +119,12 @@ __device__ __forceinline__ uint32_t scan_prefix_pipelined(const int32_t* __restr
             const uint32_t bit = (bm[a >> 5] >> (a & 31)) & 1u;
             hits += bit;
             if (kVC && bit) count_vertex(a, tri, hist);
+            if (kEC && bit) {
+                atomicAdd(&ec_c[i], 1u);
+                atomicAdd(&ec_b[rank_in_set(bm, sb, a)], 1u);
+            }
+        } else if (kEC && a == b) {
+            kb = (int32_t)i;
         }
         int32_t last;
         if constexpr (G == 1) last = a;
@@ -107,6 +132,10 @@ __device__ __forceinline__ uint32_t scan_prefix_pipelined(const int32_t* __restr
         if (last >= b) break;
         a = an;
         i = inext;
+    }
+    if (kEC) {
+        const uint32_t total = G == 1 ? hits : __reduce_add_sync(gmask, hits);
+        if (kb >= 0 && total) atomicAdd(&ec_c[kb], total);
     }
     return hits;
 }
@@ -118,7 +147,7 @@ __device__ __forceinline__ uint32_t scan_prefix_pipelined(const int32_t* __restr
 // (id, row offset, prefix length) is fetched 32 at a time with one coalesced
 // load and 32 independent gathers, then handed to groups of G lanes by
 // shuffles; each group scans one prefix with scan_prefix_pipelined.
-template <int K, int G, bool kVC = false>
+template <int K, int G, bool kVC = false, bool kEC = false>
 __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __restrict__ off,
                                                            const int32_t* __restrict__ adj,
                                                            const uint32_t* __restrict__ dplus,
@@ -130,7 +159,8 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
                                                            uint32_t bm_words,
                                                            unsigned long long* __restrict__ unit_cost,
                                                            const int32_t* __restrict__ unit_of,
-                                                           unsigned long long* __restrict__ tri = nullptr) {
+                                                           unsigned long long* __restrict__ tri = nullptr,
+                                                           uint32_t* __restrict__ ecnt = nullptr) {
     extern __shared__ uint32_t smem[];
     __shared__ uint32_t s_item[16];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -139,6 +169,10 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
     const int set_threads = K * 32, tis = wi * 32 + lane;
     uint32_t* bm = smem + (size_t)set * bm_words;
     uint32_t* hist = smem + (size_t)nsets * bm_words;  // kVC: kHubHist counters after the sets
+    // kEC: per set, the rank of the first pivot-set entry of every touched
+    // 256-id superblock (only those are ever read)
+    const uint32_t nsb = (bm_words + 7) / 8;
+    uint32_t* sb = smem + (size_t)nsets * bm_words + (size_t)set * nsb;
     const uint32_t zero_words = (uint32_t)nsets * bm_words + (kVC ? (uint32_t)kHubHist : 0u);
     for (uint32_t i = tid; i < zero_words; i += blockDim.x) smem[i] = 0;
     __syncthreads();
@@ -164,6 +198,7 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
         for (uint32_t k = tis; k < dp; k += set_threads) {
             const int32_t a = adj[rb + k];
             atomicOr(&bm[a >> 5], 1u << (a & 31));
+            if (kEC && (k == 0 || (adj[rb + k - 1] >> 8) != (a >> 8))) sb[a >> 8] = k;
         }
         set_sync();
         const uint64_t in0 = rb + dp + (uint64_t)I.j0;
@@ -184,7 +219,10 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
                 const uint64_t rcj = __shfl_sync(0xffffffffu, rc, src);
                 uint32_t limj = __shfl_sync(0xffffffffu, lim, src);
                 if (j >= nb) limj = 0;
-                if (kVC) {
+                if (kEC) {
+                    if (limj) cnt += scan_prefix_pipelined<G, false, true>(adj + rcj, limj, b, gl, gmask, bm, nullptr,
+                                                                           nullptr, ecnt + rcj, ecnt + rb, sb);
+                } else if (kVC) {
                     const int32_t cj = __shfl_sync(0xffffffffu, c, src);
                     if (limj) {
                         const uint32_t h = scan_prefix_pipelined<G, true>(adj + rcj, limj, b, gl, gmask, bm, tri, hist);
@@ -295,9 +333,55 @@ __device__ __forceinline__ uint32_t gallop_below_vc(const int32_t* __restrict__ 
     return c;
 }
 
+// Per-edge forms (kEC): matches add 1 to the slots of a in row c (x) and in
+// the pivot set (y); the pair's total goes to the slot of b = thr in x.
+__device__ __forceinline__ uint32_t merge_below_ec(const int32_t* __restrict__ x, uint32_t nx,
+                                                   const int32_t* __restrict__ y, uint32_t ny, int32_t thr,
+                                                   uint32_t* __restrict__ ec_x, uint32_t* __restrict__ ec_y) {
+    uint32_t i = 0, j = 0, c = 0;
+    while (i < nx && j < ny) {
+        const int32_t a = x[i], bb = y[j];
+        if (a >= thr || bb >= thr) break;
+        if (a < bb) ++i;
+        else if (a > bb) ++j;
+        else {
+            ++c;
+            atomicAdd(&ec_x[i], 1u);
+            atomicAdd(&ec_y[j], 1u);
+            ++i;
+            ++j;
+        }
+    }
+    while (i < nx && x[i] < thr) ++i;
+    if (c && i < nx) atomicAdd(&ec_x[i], c);  // x[i] == thr: thr is in x
+    return c;
+}
+
+__device__ __forceinline__ uint32_t gallop_below_ec(const int32_t* __restrict__ x, uint32_t nx,
+                                                    const int32_t* __restrict__ y, uint32_t ny, int32_t thr,
+                                                    uint32_t* __restrict__ ec_x, uint32_t* __restrict__ ec_y) {
+    uint32_t c = 0, i = 0;
+    for (; i < nx; ++i) {
+        const int32_t a = x[i];
+        if (a >= thr) break;
+        uint32_t lo = 0, hi = ny;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (y[mid] < a) lo = mid + 1; else hi = mid;
+        }
+        if (lo < ny && y[lo] == a) {
+            ++c;
+            atomicAdd(&ec_x[i], 1u);
+            atomicAdd(&ec_y[lo], 1u);
+        }
+    }
+    if (c && i < nx) atomicAdd(&ec_x[i], c);
+    return c;
+}
+
 // Warp kernels: one item (pivot, <= kChunkWarp in-neighbours) per warp, one
 // lane per in-neighbour.
-template <int MODE, bool kVC = false>
+template <int MODE, bool kVC = false, bool kEC = false>
 __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* __restrict__ off,
                                                                 const int32_t* __restrict__ adj,
                                                                 const uint32_t* __restrict__ dplus,
@@ -308,11 +392,14 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
                                                                 unsigned long long* __restrict__ total,
                                                                 unsigned long long* __restrict__ unit_cost,
                                                                 const int32_t* __restrict__ unit_of,
-                                                                unsigned long long* __restrict__ tri = nullptr) {
+                                                                unsigned long long* __restrict__ tri = nullptr,
+                                                                uint32_t* __restrict__ ecnt = nullptr) {
     __shared__ int32_t table[MODE == kModeHash ? kWarpCtaWarps : 1][MODE == kModeHash ? kHashSlots : 1];
+    __shared__ int32_t tpos[MODE == kModeHash && kEC ? kWarpCtaWarps : 1][MODE == kModeHash && kEC ? kHashSlots : 1];
     __shared__ uint32_t hist[kVC ? kHubHist : 1];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int32_t* T = table[MODE == kModeHash ? w : 0];
+    int32_t* TP = tpos[MODE == kModeHash && kEC ? w : 0];  // kEC: position of each key in N+(b)
     if (kVC) {
         for (int i = threadIdx.x; i < kHubHist; i += blockDim.x) hist[i] = 0;
         __syncthreads();
@@ -342,14 +429,16 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
                 const int32_t a = nb[k];
                 uint32_t s = hash_slot(a);
                 while (atomicCAS(&T[s], -1, a) != -1) s = (s + 1) & (kHashSlots - 1);
+                if (kEC) TP[s] = (int32_t)k;
             }
             __syncwarp();
             for (uint64_t e = in0 + lane; e < in1; e += 32) {
                 const int32_t c = adj[e];
-                const int32_t* row = adj + off[c];
+                const uint64_t rc = off[c];
+                const int32_t* row = adj + rc;
                 const uint32_t lim = dplus[c];
-                uint32_t h = 0;
-                for (uint32_t i = 0; i < lim; ++i) {
+                uint32_t h = 0, i = 0;
+                for (; i < lim; ++i) {
                     const int32_t a = __ldg(row + i);
                     if (a >= b) break;
                     uint32_t s = hash_slot(a);
@@ -358,6 +447,10 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
                         if (key == a) {
                             ++h;
                             if (kVC) count_vertex(a, tri, hist);
+                            if (kEC) {
+                                atomicAdd(&ecnt[rc + i], 1u);
+                                atomicAdd(&ecnt[rb + TP[s]], 1u);
+                            }
                             break;
                         }
                         s = (s + 1) & (kHashSlots - 1);
@@ -365,6 +458,7 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
                 }
                 cnt += h;
                 if (kVC && h) atomicAdd(&tri[c], (unsigned long long)h);
+                if (kEC && h && i < lim) atomicAdd(&ecnt[rc + i], h);  // row[i] == b
             }
             __syncwarp();
             for (int s = lane; s < kHashSlots; s += 32) T[s] = -1;
@@ -372,6 +466,11 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
         } else if (MODE == kModeGallop) {
             for (uint64_t e = in0 + lane; e < in1; e += 32) {
                 const int32_t c = adj[e];
+                if (kEC) {
+                    const uint64_t rc = off[c];
+                    cnt += gallop_below_ec(adj + rc, dplus[c], nb, dp, b, ecnt + rc, ecnt + rb);
+                    continue;
+                }
                 const uint32_t h = gallop_below_vc<kVC>(adj + off[c], dplus[c], nb, dp, b, tri, hist);
                 cnt += h;
                 if (kVC && h) atomicAdd(&tri[c], (unsigned long long)h);
@@ -379,6 +478,11 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
         } else {
             for (uint64_t e = in0 + lane; e < in1; e += 32) {
                 const int32_t c = adj[e];
+                if (kEC) {
+                    const uint64_t rc = off[c];
+                    cnt += merge_below_ec(adj + rc, dplus[c], nb, dp, b, ecnt + rc, ecnt + rb);
+                    continue;
+                }
                 const uint32_t h = merge_below_vc<kVC>(adj + off[c], dplus[c], nb, dp, b, tri, hist);
                 cnt += h;
                 if (kVC && h) atomicAdd(&tri[c], (unsigned long long)h);
