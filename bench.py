@@ -274,7 +274,8 @@ def run_reference_arm(args, dist):
 
 def train_selector(pc, args):
     """Training data generated by the method itself on separate graphs (RMAT
-    at two scales with other seeds, ER and Chung-Lu): in-situ per-unit costs
+    at three scales with other seeds than the measured graph, ER and
+    Chung-Lu): in-situ per-unit costs
     of every variant, one collection group per graph; the heuristic is
     autotuned on the samples, then the MLP is trained on the GPU with its
     judge margin chosen by leave-one-graph-out validation."""
@@ -283,7 +284,7 @@ def train_selector(pc, args):
     s = args.train_scale
     graphs = [lambda: pc.Graph.rmat_device(s - 2, args.edge_factor, args.seed + 4),
               lambda: pc.Graph.rmat_device(s, args.edge_factor, args.seed + 1),
-              lambda: pc.Graph.rmat_device(s + 1, args.edge_factor, args.seed + 5),
+              lambda: pc.Graph.rmat_device(s + 2, args.edge_factor, args.seed + 5),
               lambda: pc.Graph.er_device(s - 2, 1 << (s + 2), args.seed + 2),
               lambda: pc.Graph(host=pc.HostCSR.chung_lu(s - 2, 1 << (s + 2), 2.1, 1 << (s - 6), args.seed + 3))]
     for make in graphs:
