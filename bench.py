@@ -678,7 +678,16 @@ def suite_selector_graph(pc, O, torch, args, emit, name, h, P, suite):
     lp["unit_cost_sums"] = plan_bounds(pc, pg)
     peak, peak_kind = hbm_peak()
     kms = lp["learned_ms"]
+    # all-edge Jaccard runs the triangle kernels in per-edge mode under the
+    # same plan: learned (selector on) and plain (selector off), same output
     t_j, jac = _timed(lambda: pg.jaccard_edges(), max(1, args.steps // 2), 1)
+    pc.selector.enable(False)
+    try:
+        t_jp, jac_p = _timed(lambda: pg.jaccard_edges(), max(1, args.steps // 2), 1)
+    finally:
+        pc.selector.enable(True)
+    if not np.array_equal(jac, jac_p):
+        raise SystemExit("Jaccard differs between the learned and the plain plan")
     # Jaccard spot check: the oracle's formula on a sample of rows
     rows = np.arange(0, n, max(1, n // 500), dtype=np.int64)
     bad = 0
@@ -696,7 +705,8 @@ def suite_selector_graph(pc, O, torch, args, emit, name, h, P, suite):
     emit({"suite": suite, "workload": f"{name}_p{P}", "n": int(n), "m_directed": int(m), **lp,
           "tc_gteps_learned": round(e_plus / (kms / 1e3) / 1e9, 4),
           "tc_roofline_frac": round(algo_bytes / (kms / 1e3) / 1e9 / peak, 4), "peak_kind": peak_kind,
-          "W": int(W), "jaccard_ms": round(t_j * 1e3, 3), "jaccard_gteps": round(m / t_j / 1e9, 4),
+          "W": int(W), "jaccard_ms": round(t_j * 1e3, 3), "jaccard_plain_ms": round(t_jp * 1e3, 3),
+          "jaccard_speedup": round(t_jp / t_j, 4), "jaccard_gteps": round(m / t_j / 1e9, 4),
           "jaccard_spot_mismatches": bad,
           "cpu_tc_gteps": gteps_cpu, "cpu_kind": kind, "cpu_cores": os.cpu_count(), "cpu_sample": sample})
     pg.close()

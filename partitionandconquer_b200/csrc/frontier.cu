@@ -192,56 +192,109 @@ __global__ void k_kcore_init(const uint64_t* __restrict__ off, uint64_t n, int32
     rem[u] = (int32_t)u;
 }
 
-// Scan of the remaining vertices at level k: degree < k -> core k-1, into the
-// peel queue; others stay (compacted).  Also returns the minimum degree left.
-__global__ void k_kcore_scan(const int32_t* __restrict__ rem, uint32_t rn, int32_t k, int32_t* __restrict__ deg,
-                             int32_t* __restrict__ core, int32_t* __restrict__ fq, uint32_t* __restrict__ fn,
-                             int32_t* __restrict__ rem2, uint32_t* __restrict__ rn2, int32_t* __restrict__ min_left) {
+// Device-driven peeling.  One launch is one step: a peel round at the current
+// level when the frontier is not empty, else the scan of the next level.  The
+// state lives in three rotating records: step i reads S[i % 3], accumulates
+// into S[(i+1) % 3] (counters prepared by step i-1) and prepares S[(i+2) % 3],
+// which nobody else touches while step i runs.  The host enqueues steps in
+// batches and reads the done flag once per batch, instead of synchronising
+// after every scan and every peel round.
+struct KState {
+    int32_t k;      // level of the step that wrote this record
+    uint32_t fn;    // frontier size it produced
+    uint32_t rn;    // remaining (unpeeled) vertices after it
+    int32_t ml;     // minimum degree left (scan steps)
+    int32_t phase;  // 0 scan, 1 peel
+    int32_t fpar;   // frontier buffer holding the frontier
+    int32_t rpar;   // remaining-list buffer
+    int32_t done;
+};
+
+__global__ void k_kcore_step(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj, uint64_t n,
+                             int32_t* __restrict__ deg, int32_t* __restrict__ core, int32_t* __restrict__ rem0,
+                             int32_t* __restrict__ rem1, int32_t* __restrict__ f0, int32_t* __restrict__ f1,
+                             KState* __restrict__ S, uint32_t step) {
+    const KState in = S[step % 3];
+    KState* out = &S[(step + 1) % 3];
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    if (lead) {  // prepare the record step+1 accumulates into
+        KState* clr = &S[(step + 2) % 3];
+        clr->fn = 0;
+        clr->rn = 0;
+        clr->ml = INT_MAX;
+    }
+    bool peel;
+    int32_t k;
+    if (in.done) {
+        peel = false;
+        k = in.k;
+    } else if (in.fn > 0) {
+        peel = true;
+        k = in.k;
+    } else {
+        peel = false;
+        k = (in.phase == 1 || in.ml == INT_MAX) ? in.k + 1 : max(in.k + 1, in.ml + 1);
+    }
+    const bool done = in.done || (!peel && (in.rn == 0 || (uint64_t)k >= n));
+    if (threadIdx.x == 0) {  // every CTA writes the same values
+        out->k = k;
+        out->phase = peel ? 1 : 0;
+        out->done = done ? 1 : 0;
+        out->fpar = peel ? 1 - in.fpar : 0;
+        out->rpar = peel ? in.rpar : 1 - in.rpar;
+    }
+    if (done) {
+        if (lead) out->rn = in.rn;
+        return;
+    }
+    if (peel) {
+        if (lead) out->rn = in.rn;
+        const int32_t* fq = in.fpar ? f1 : f0;
+        int32_t* nq = in.fpar ? f0 : f1;
+        const int lane = threadIdx.x & 31;
+        const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+        const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+        for (uint64_t i = warp; i < in.fn; i += nwarps) {
+            const int32_t u = fq[i];
+            const uint64_t b = off[u], e = off[u + 1];
+            for (uint64_t j0 = b; j0 < e; j0 += 32) {
+                const uint64_t j = j0 + lane;
+                bool push = false;
+                int32_t v = 0;
+                if (j < e) {
+                    v = adj[j];
+                    if (core[v] < 0) {
+                        const int32_t old = atomicSub(&deg[v], 1);
+                        if (old == k) { push = true; core[v] = k - 1; }
+                    }
+                }
+                warp_append(push, v, nq, &out->fn);
+            }
+        }
+        return;
+    }
+    // scan of level k over the remaining list
+    const int32_t* rem = in.rpar ? rem1 : rem0;
+    int32_t* rem2 = in.rpar ? rem0 : rem1;
+    const uint32_t rn = in.rn;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t nr = (rn + 31) & ~31u;
     int32_t mn = INT_MAX;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nr; i += stride) {
-        bool peel = false, keep = false;
+        bool pl = false, keep = false;
         int32_t u = 0;
         if (i < rn) {
             u = rem[i];
             if (core[u] < 0) {
-                if (deg[u] < k) { peel = true; core[u] = k - 1; }
+                if (deg[u] < k) { pl = true; core[u] = k - 1; }
                 else { keep = true; mn = min(mn, deg[u]); }
             }
         }
-        warp_append(peel, u, fq, fn);
-        warp_append(keep, u, rem2, rn2);
+        warp_append(pl, u, f0, &out->fn);
+        warp_append(keep, u, rem2, &out->rn);
     }
     for (int o = 16; o; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-    if ((threadIdx.x & 31) == 0 && mn != INT_MAX) atomicMin(min_left, mn);
-}
-
-// Peeling step: neighbours of peeled vertices lose one degree; a neighbour
-// whose degree crosses from k to k-1 is peeled next (exactly once).
-__global__ void k_kcore_peel(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
-                             const int32_t* __restrict__ fq, uint32_t fn, int32_t k, int32_t* __restrict__ deg,
-                             int32_t* __restrict__ core, int32_t* __restrict__ nq, uint32_t* __restrict__ nn) {
-    const int lane = threadIdx.x & 31;
-    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t i = warp; i < fn; i += nwarps) {
-        const int32_t u = fq[i];
-        const uint64_t b = off[u], e = off[u + 1];
-        for (uint64_t j0 = b; j0 < e; j0 += 32) {
-            const uint64_t j = j0 + lane;
-            bool push = false;
-            int32_t v = 0;
-            if (j < e) {
-                v = adj[j];
-                if (core[v] < 0) {
-                    const int32_t old = atomicSub(&deg[v], 1);
-                    if (old == k) { push = true; core[v] = k - 1; }
-                }
-            }
-            warp_append(push, v, nq, nn);
-        }
-    }
+    if ((threadIdx.x & 31) == 0 && mn != INT_MAX) atomicMin(&out->ml, mn);
 }
 
 __global__ void k_kcore_unpeeled(int32_t* __restrict__ core, uint64_t n) {
@@ -544,67 +597,60 @@ pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
         if (largest) *largest = 0;
         return PC_OK;
     }
-    PC_TRY(scratch_reserve(pg, n * 4 * 7 + 1024));
+    PC_TRY(scratch_reserve(pg, n * 4 * 7 + sizeof(KState) * 3));
     int32_t* deg = pg->scratch.take<int32_t>(n);
     int32_t* core = pg->scratch.take<int32_t>(n);
-    int32_t* rem = pg->scratch.take<int32_t>(n);
-    int32_t* rem2 = pg->scratch.take<int32_t>(n);
+    int32_t* rem0 = pg->scratch.take<int32_t>(n);
+    int32_t* rem1 = pg->scratch.take<int32_t>(n);
     int32_t* f0 = pg->scratch.take<int32_t>(n);
     int32_t* f1 = pg->scratch.take<int32_t>(n);
     int32_t* out = pg->scratch.take<int32_t>(n);
-    uint32_t* cnt = pg->scratch.take<uint32_t>(4);  // 0 frontier, 1 remaining, 2 next frontier
-    int32_t* minleft = pg->scratch.take<int32_t>(1);
+    KState* S = pg->scratch.take<KState>(3);
+    if (!S) return fail(PC_ERR_OOM, "k-core scratch plan exceeds its reservation");
     const unsigned nb = (unsigned)ceil_div(n, kThreads);
-    k_kcore_init<<<nb, kThreads, 0, s>>>(pg->off, n, deg, core, rem);
+    k_kcore_init<<<nb, kThreads, 0, s>>>(pg->off, n, deg, core, rem0);
     PC_LAUNCHED();
-    uint32_t rn = (uint32_t)n;
-    int32_t k = 1, top = 0;
-    // Levels k = 1 .. n-1, as the reference's loop (src/Graph.cpp:683, 1893);
-    // vertices never peeled (only in a complete graph) keep core 0.
-    while (rn > 0 && (uint64_t)k < n) {
-        // level k: peel every remaining vertex of degree < k (src/Graph.cpp:683-717)
-        PC_CUDA(cudaMemsetAsync(cnt, 0, 16, s));
-        const int32_t big = INT_MAX;
-        PC_CUDA(cudaMemcpyAsync(minleft, &big, 4, cudaMemcpyHostToDevice, s));
-        k_kcore_scan<<<(unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(rn, kThreads), grid_for(pg, 16))),
-                       kThreads, 0, s>>>(rem, rn, k, deg, core, f0, cnt, rem2, cnt + 1, minleft);
-        PC_LAUNCHED();
-        uint32_t h[2];
-        int32_t ml = 0;
-        PC_CUDA(cudaMemcpyAsync(h, cnt, 8, cudaMemcpyDeviceToHost, s));
-        PC_CUDA(cudaMemcpyAsync(&ml, minleft, 4, cudaMemcpyDeviceToHost, s));
-        PC_CUDA(cudaStreamSynchronize(s));
-        uint32_t fn = h[0];
-        std::swap(rem, rem2);
-        rn = h[1];
-        if (fn == 0) {
-            // Nothing below k: every remaining degree is >= ml (read with no
-            // peeling in flight), so levels k..ml are empty; the reference
-            // makes the same jump (src/Graph.cpp:1921).
-            if (rn == 0) break;
-            k = (int32_t)std::min<int64_t>(std::max<int64_t>((int64_t)k + 1, (int64_t)ml + 1), (int64_t)n);
-            continue;
-        }
-        top = k - 1;
-        int32_t* fq = f0;
-        int32_t* nq = f1;
-        while (fn > 0) {
-            PC_CUDA(cudaMemsetAsync(cnt + 2, 0, 4, s));
-            k_kcore_peel<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, fq, fn, k, deg, core, nq, cnt + 2);
+    // Levels k = 1 .. n-1, as the reference's loop (src/Graph.cpp:683, 1893):
+    // at level k every remaining vertex of degree < k gets core k-1, and
+    // peeling repeats until no degree crosses below k; empty levels jump to
+    // the minimum degree left, as the reference does (src/Graph.cpp:1921).
+    // Vertices never peeled (only in a complete graph) keep core 0.
+    KState init[3] = {};
+    init[0].k = 0;
+    init[0].fn = 0;
+    init[0].rn = (uint32_t)n;
+    init[0].ml = 0;
+    init[0].phase = 0;
+    init[0].rpar = 0;
+    init[1].ml = INT_MAX;
+    PC_CUDA(cudaMemcpyAsync(S, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    const unsigned grid = grid_for(pg, 8);
+    constexpr uint32_t kBatch = 32;
+    // every step either peels (shrinking the degrees) or advances the level,
+    // so n levels plus n peel rounds bound the steps
+    const uint64_t max_steps = 2 * n + 8;
+    uint32_t step = 0;
+    for (;;) {
+        for (uint32_t i = 0; i < kBatch; ++i, ++step) {
+            k_kcore_step<<<grid, kThreads, 0, s>>>(pg->off, pg->adj, n, deg, core, rem0, rem1, f0, f1, S, step);
             PC_LAUNCHED();
-            PC_TRY(read_u32(pg, cnt + 2, &fn));
-            std::swap(fq, nq);
         }
-        // peeling may have pushed kept vertices down to exactly k: rescan at k+1
-        ++k;
+        int32_t done = 0;
+        PC_CUDA(cudaMemcpyAsync(&done, &S[step % 3].done, 4, cudaMemcpyDeviceToHost, s));
+        PC_CUDA(cudaStreamSynchronize(s));
+        if (done) break;
+        if (step > max_steps) return fail(PC_ERR_TIMEOUT, "k-core peeling did not finish");
     }
     k_kcore_unpeeled<<<nb, kThreads, 0, s>>>(core, n);
     PC_LAUNCHED();
-    // vertices kept in `rem` may have been peeled after the scan: all have core >= 0 now
     PC_TRY(gather_to_api_i32(pg, core, out));
     PC_CUDA(cudaMemcpyAsync(core_host, out, n * 4, cudaMemcpyDeviceToHost, s));
     PC_TRY(sync(pg));
-    if (largest) *largest = top;
+    if (largest) {
+        int32_t top = 0;
+        for (uint64_t u = 0; u < n; ++u) top = std::max(top, core_host[u]);
+        *largest = top;
+    }
     return PC_OK;
 }
 

@@ -32,10 +32,10 @@ void features_to_inputs(const float* f, float* x);
 struct HeuristicParams {
     // Defaults: the thresholds pc_selector_autotune chose from in-situ unit
     // costs of RMAT graphs at scales 20, 22 and 24 (with ER and Chung-Lu).
-    double min_in_per_pivot_cta = 64.0;  // in-edges per pivot to use a bitmap form
-    double warp_scan = 192.0;            // mean prefix bound for 32 lanes per in-neighbour
-    double group_scan = 0.0;             // ... for 8 lanes per in-neighbour
-    double matrix_scan = 192.0;          // ... for the in-neighbour-major hub form (ids < 2^16)
+    double min_in_per_pivot_cta = 128.0;  // in-edges per pivot to use a bitmap form
+    double warp_scan = 256.0;             // mean prefix bound for 32 lanes per in-neighbour
+    double group_scan = 0.0;              // ... for 8 lanes per in-neighbour
+    double matrix_scan = 256.0;           // ... for the in-neighbour-major hub form (ids < 2^16)
 };
 HeuristicParams heuristic_params();
 void set_heuristic_params(const HeuristicParams& hp);
