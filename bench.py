@@ -210,7 +210,7 @@ class ClockSampler:
 
 # ---- the reference arm ----------------------------------------------------------
 
-def reference_tc_sample(vl, el, target_s, threads):
+def reference_tc_sample(vl, el, target_s, threads, graph=None):
     """Times the reference's TC loop on every k-th row; returns (GTEPS, sample)."""
     from oracle import oracle as O
     n = vl.size - 1
@@ -234,7 +234,7 @@ def reference_tc_sample(vl, el, target_s, threads):
         k = max(1, int(k * max(dt, 1e-3) / target_s * 1.5)) if dt > 0.05 else max(1, k // 16)
     gteps = e_plus / (dt * k) / 1e9
     sample = (f"the reference's TC loop (body and static OpenMP schedule of Graph::solve_triangle_counting_merge) "
-              f"over rows u = 0 mod {k} ({rows.size} of {n} rows) of the RMAT-{int(np.log2(n))} graph, "
+              f"over rows u = 0 mod {k} ({rows.size} of {n} rows) of the {graph or f'RMAT-{int(np.log2(n))}'} graph, "
               f"{dt:.2f} s, extrapolated x{k}")
     return gteps, kind, sample, R, run, rows, k, e_plus
 
@@ -699,7 +699,7 @@ def suite_selector_graph(pc, O, torch, args, emit, name, h, P, suite):
             want = np.float32(c / (deg[u] + deg[v] - c))
             if jac[vl[u] + k] != want:
                 bad += 1
-    gteps_cpu, kind, sample, Rf, *_ = reference_tc_sample(vl, el, args.cpu_sample_seconds, os.cpu_count() or 1)
+    gteps_cpu, kind, sample, Rf, *_ = reference_tc_sample(vl, el, args.cpu_sample_seconds, os.cpu_count() or 1, name)
     if Rf is not None:
         Rf.close()
     emit({"suite": suite, "workload": f"{name}_p{P}", "n": int(n), "m_directed": int(m), **lp,

@@ -64,6 +64,14 @@ pc_status pc_release_cached_memory(void);
 /* Page-lock (or release) a caller buffer so host<->device copies are DMA. */
 pc_status pc_host_register(void* ptr, size_t bytes);
 pc_status pc_host_unregister(void* ptr);
+/* Self-test of the bounded grid barrier that the persistent kernels (k-core)
+ * use: `rounds` barriers over a cooperative grid on `device`, checking that
+ * no CTA passes a barrier early (*mismatches counts violations, 0 expected).
+ * With absent_cta >= 0 that CTA never arrives: the other CTAs' waits run out
+ * after limit_ms and the call returns PC_ERR_TIMEOUT with the device still
+ * usable.  Not part of the reference interface; a diagnostic. */
+pc_status pc_selftest_grid_barrier(int32_t device, int32_t rounds, int32_t absent_cta, uint32_t limit_ms,
+                                   uint32_t* mismatches);
 
 /* ---- graph (class Graph, src/Graph.hpp:38-103) ------------------------- */
 

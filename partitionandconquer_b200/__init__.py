@@ -37,6 +37,16 @@ def launch_count() -> int:
     return int(lib.pc_launch_count())
 
 
+def selftest_grid_barrier(device: int = 0, rounds: int = 64, absent_cta: int = -1, limit_ms: int = 1000) -> int:
+    """Runs the bounded grid barrier of the persistent kernels `rounds` times
+    and returns the number of ordering violations seen (0 expected).  With
+    absent_cta >= 0 one CTA never arrives and PCError (status TIMEOUT) is
+    raised once the others' waits run out."""
+    bad = C.c_uint32(0)
+    check(lib.pc_selftest_grid_barrier(device, rounds, absent_cta, limit_ms, C.byref(bad)))
+    return int(bad.value)
+
+
 def vertex_priority(seed: int, n: int) -> np.ndarray:
     """Priorities Partitioned_Graph.solve_mis(seed=...) orders vertices by."""
     out = np.empty(n, np.uint64)
@@ -441,8 +451,17 @@ class Partitioned_Graph:
     def solve_lcc_galloping(self):
         return self._lcc(METHOD_GALLOPING)
 
-    def jaccard_edges(self):
-        out = np.empty(self.get_edge_num(), np.float32)
+    def jaccard_edges(self, out=None):
+        """J per CSR entry (fp32).  `out`, when given, is a C-contiguous float32
+        host array of get_edge_num() entries that receives the values; pinned
+        memory (e.g. a pinned torch tensor's .numpy()) makes the copy back run
+        at DMA speed instead of being staged through the driver."""
+        m = self.get_edge_num()
+        if out is None:
+            out = np.empty(m, np.float32)
+        elif (not isinstance(out, np.ndarray) or out.dtype != np.float32 or out.size != m
+              or not out.flags.c_contiguous or not out.flags.writeable):
+            raise ValueError(f"out must be a writeable C-contiguous float32 array of {m} entries")
         check(lib.pc_jaccard_edges(self._pg, ptr(out)))
         return out
 

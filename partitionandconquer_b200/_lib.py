@@ -83,6 +83,7 @@ _SIG = {
     "pc_launch_count": (u64, []),
     "pc_host_register": (i32, [P, C.c_size_t]),
     "pc_release_cached_memory": (i32, []),
+    "pc_selftest_grid_barrier": (i32, [i32, i32, i32, u32, P]),
     "pc_host_unregister": (i32, [P]),
     "pc_graph_create": (i32, [P, P, P, u64, u64, u32, PP]),
     "pc_graph_destroy": (i32, [P]),

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <vector>
 
+#include "grid_sync.cuh"
 #include "pc_internal.cuh"
 #include "synth_rng.h"
 
@@ -17,6 +18,8 @@ namespace fr {
 
 constexpr int kThreads = 256;
 constexpr int32_t kInf = INT_MAX;
+// bound on any grid-barrier wait of the persistent kernels (4 s)
+constexpr uint64_t kBarrierLimitNs = 4000000000ull;
 
 // Appends `val` for every lane with pred set; all 32 lanes of the warp must
 // call it together.
@@ -192,13 +195,13 @@ __global__ void k_kcore_init(const uint64_t* __restrict__ off, uint64_t n, int32
     rem[u] = (int32_t)u;
 }
 
-// Device-driven peeling.  One launch is one step: a peel round at the current
-// level when the frontier is not empty, else the scan of the next level.  The
-// state lives in three rotating records: step i reads S[i % 3], accumulates
-// into S[(i+1) % 3] (counters prepared by step i-1) and prepares S[(i+2) % 3],
-// which nobody else touches while step i runs.  The host enqueues steps in
-// batches and reads the done flag once per batch, instead of synchronising
-// after every scan and every peel round.
+// Device-driven peeling in one persistent kernel.  Each step is a peel round
+// at the current level when the frontier is not empty, else the scan of the
+// next level; a grid barrier separates steps.  The state lives in three
+// rotating records: step i reads S[i % 3], accumulates into S[(i+1) % 3]
+// (counters cleared by step i-1) and clears S[(i+2) % 3], which no CTA reads
+// during step i.  Mutable arrays are read with __ldcg: L1 is not coherent
+// across CTAs within one launch.
 struct KState {
     int32_t k;      // level of the step that wrote this record
     uint32_t fn;    // frontier size it produced
@@ -207,94 +210,125 @@ struct KState {
     int32_t phase;  // 0 scan, 1 peel
     int32_t fpar;   // frontier buffer holding the frontier
     int32_t rpar;   // remaining-list buffer
-    int32_t done;
+    int32_t pad;
 };
 
-__global__ void k_kcore_step(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj, uint64_t n,
-                             int32_t* __restrict__ deg, int32_t* __restrict__ core, int32_t* __restrict__ rem0,
-                             int32_t* __restrict__ rem1, int32_t* __restrict__ f0, int32_t* __restrict__ f1,
-                             KState* __restrict__ S, uint32_t step) {
-    const KState in = S[step % 3];
-    KState* out = &S[(step + 1) % 3];
+__device__ __forceinline__ KState load_state(const KState* p) {
+    const int4 lo = __ldcg(reinterpret_cast<const int4*>(p));
+    const int4 hi = __ldcg(reinterpret_cast<const int4*>(p) + 1);
+    KState s;
+    s.k = lo.x;
+    s.fn = (uint32_t)lo.y;
+    s.rn = (uint32_t)lo.z;
+    s.ml = lo.w;
+    s.phase = hi.x;
+    s.fpar = hi.y;
+    s.rpar = hi.z;
+    s.pad = hi.w;
+    return s;
+}
+
+__global__ void __launch_bounds__(kThreads) k_kcore_persistent(
+    const uint64_t* __restrict__ off, const int32_t* __restrict__ adj, uint64_t n, int32_t* deg, int32_t* core,
+    int32_t* rem0, int32_t* rem1, int32_t* f0, int32_t* f1, KState* S, GridBarrier* gb, uint64_t max_steps,
+    uint64_t limit_ns, uint64_t* steps_done) {
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
-    if (lead) {  // prepare the record step+1 accumulates into
-        KState* clr = &S[(step + 2) % 3];
-        clr->fn = 0;
-        clr->rn = 0;
-        clr->ml = INT_MAX;
-    }
-    bool peel;
-    int32_t k;
-    if (in.done) {
-        peel = false;
-        k = in.k;
-    } else if (in.fn > 0) {
-        peel = true;
-        k = in.k;
-    } else {
-        peel = false;
-        k = (in.phase == 1 || in.ml == INT_MAX) ? in.k + 1 : max(in.k + 1, in.ml + 1);
-    }
-    const bool done = in.done || (!peel && (in.rn == 0 || (uint64_t)k >= n));
-    if (threadIdx.x == 0) {  // every CTA writes the same values
-        out->k = k;
-        out->phase = peel ? 1 : 0;
-        out->done = done ? 1 : 0;
-        out->fpar = peel ? 1 - in.fpar : 0;
-        out->rpar = peel ? in.rpar : 1 - in.rpar;
-    }
-    if (done) {
-        if (lead) out->rn = in.rn;
-        return;
-    }
-    if (peel) {
-        if (lead) out->rn = in.rn;
-        const int32_t* fq = in.fpar ? f1 : f0;
-        int32_t* nq = in.fpar ? f0 : f1;
-        const int lane = threadIdx.x & 31;
-        const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-        const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-        for (uint64_t i = warp; i < in.fn; i += nwarps) {
-            const int32_t u = fq[i];
-            const uint64_t b = off[u], e = off[u + 1];
-            for (uint64_t j0 = b; j0 < e; j0 += 32) {
-                const uint64_t j = j0 + lane;
-                bool push = false;
-                int32_t v = 0;
-                if (j < e) {
-                    v = adj[j];
-                    if (core[v] < 0) {
-                        const int32_t old = atomicSub(&deg[v], 1);
-                        if (old == k) { push = true; core[v] = k - 1; }
+    const int lane = threadIdx.x & 31;
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t warp = tid >> 5, nwarps = stride >> 5;
+    uint64_t step = 0;
+    for (; step < max_steps; ++step) {
+        const KState in = load_state(&S[step % 3]);
+        KState* out = &S[(step + 1) % 3];
+        const bool peel = in.fn > 0;
+        const int32_t k = peel ? in.k
+                               : ((in.phase == 1 || in.ml == INT_MAX) ? in.k + 1 : max(in.k + 1, in.ml + 1));
+        // every CTA reads the same record, so all leave at the same step
+        if (!peel && (in.rn == 0 || (uint64_t)k >= n)) break;
+        if (lead) {
+            KState* clr = &S[(step + 2) % 3];
+            clr->fn = 0;
+            clr->rn = 0;
+            clr->ml = INT_MAX;
+            if (peel) out->rn = in.rn;  // a peel round keeps the remaining list
+            out->k = k;
+            out->phase = peel ? 1 : 0;
+            out->fpar = peel ? 1 - in.fpar : 0;
+            out->rpar = peel ? in.rpar : 1 - in.rpar;
+        }
+        if (peel) {
+            const int32_t* fq = in.fpar ? f1 : f0;
+            int32_t* nq = in.fpar ? f0 : f1;
+            for (uint64_t i = warp; i < in.fn; i += nwarps) {
+                const int32_t u = __ldcg(fq + i);
+                const uint64_t b = off[u], e = off[u + 1];
+                for (uint64_t j0 = b; j0 < e; j0 += 32) {
+                    const uint64_t j = j0 + lane;
+                    bool push = false;
+                    int32_t v = 0;
+                    if (j < e) {
+                        v = adj[j];
+                        if (__ldcg(core + v) < 0) {
+                            const int32_t old = atomicSub(&deg[v], 1);
+                            if (old == k) {
+                                push = true;
+                                core[v] = k - 1;
+                            }
+                        }
+                    }
+                    warp_append(push, v, nq, &out->fn);
+                }
+            }
+        } else {
+            // scan of level k over the remaining list
+            const int32_t* rem = in.rpar ? rem1 : rem0;
+            int32_t* rem2 = in.rpar ? rem0 : rem1;
+            const uint64_t nr = ((uint64_t)in.rn + 31) & ~(uint64_t)31;
+            int32_t mn = INT_MAX;
+            for (uint64_t i = tid; i < nr; i += stride) {
+                bool pl = false, keep = false;
+                int32_t u = 0;
+                if (i < in.rn) {
+                    u = __ldcg(rem + i);
+                    if (__ldcg(core + u) < 0) {
+                        const int32_t d = __ldcg(deg + u);
+                        if (d < k) {
+                            pl = true;
+                            core[u] = k - 1;
+                        } else {
+                            keep = true;
+                            mn = min(mn, d);
+                        }
                     }
                 }
-                warp_append(push, v, nq, &out->fn);
+                warp_append(pl, u, f0, &out->fn);
+                warp_append(keep, u, rem2, &out->rn);
             }
+            for (int o = 16; o; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+            if (lane == 0 && mn != INT_MAX) atomicMin(&out->ml, mn);
         }
-        return;
+        if (!grid_sync(gb, limit_ns)) return;
     }
-    // scan of level k over the remaining list
-    const int32_t* rem = in.rpar ? rem1 : rem0;
-    int32_t* rem2 = in.rpar ? rem0 : rem1;
-    const uint32_t rn = in.rn;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t nr = (rn + 31) & ~31u;
-    int32_t mn = INT_MAX;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nr; i += stride) {
-        bool pl = false, keep = false;
-        int32_t u = 0;
-        if (i < rn) {
-            u = rem[i];
-            if (core[u] < 0) {
-                if (deg[u] < k) { pl = true; core[u] = k - 1; }
-                else { keep = true; mn = min(mn, deg[u]); }
-            }
-        }
-        warp_append(pl, u, f0, &out->fn);
-        warp_append(keep, u, rem2, &out->rn);
+    if (lead) {
+        *steps_done = step;
+        if (step == max_steps) atomicExch(&gb->err, 2);
     }
-    for (int o = 16; o; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-    if ((threadIdx.x & 31) == 0 && mn != INT_MAX) atomicMin(&out->ml, mn);
+}
+
+// Self-test of the grid barrier: `rounds` barriers, each CTA adding 1 to
+// `tally` before each; CTA `absent` (if >= 0) never arrives, so the others'
+// waits run out after limit_ns and the barrier reports it.
+__global__ void k_grid_sync_selftest(GridBarrier* gb, int rounds, int absent, uint64_t limit_ns,
+                                     unsigned* tally, unsigned* bad) {
+    if ((int)blockIdx.x == absent) return;
+    for (int r = 0; r < rounds; ++r) {
+        if (threadIdx.x == 0) atomicAdd(tally, 1u);
+        if (!grid_sync(gb, limit_ns)) return;
+        // after barrier r every CTA has added its r+1 increments
+        if (threadIdx.x == 0 && __ldcg(tally) < (unsigned)(r + 1) * gridDim.x) atomicAdd(bad, 1u);
+        if (!grid_sync(gb, limit_ns)) return;
+    }
 }
 
 __global__ void k_kcore_unpeeled(int32_t* __restrict__ core, uint64_t n) {
@@ -587,6 +621,45 @@ pc_status pc_pagerank_f64(pc_pgraph* pg, double damping, int32_t iterations, con
     return pagerank_run<double>(pg, damping, iterations, init, out);
 }
 
+pc_status pc_selftest_grid_barrier(int32_t device, int32_t rounds, int32_t absent_cta, uint32_t limit_ms,
+                                   uint32_t* mismatches) {
+    clear_error();
+    if (rounds < 0 || !mismatches || limit_ms == 0) return fail(PC_ERR_INVALID_INPUT, "bad argument");
+    PC_TRY(pc_set_device(device));
+    int per_sm = 0;
+    PC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_sync_selftest, kThreads, 0));
+    if (per_sm < 1) return fail(PC_ERR_CUDA, "self-test kernel cannot be resident");
+    const int grid = sm_count(device) * std::min(per_sm, 2);
+    if (absent_cta >= grid) return fail(PC_ERR_INVALID_INPUT, "absent_cta is outside the grid");
+    cudaStream_t s = nullptr;
+    PC_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    DevBuf buf;
+    pc_status st = buf.alloc(sizeof(GridBarrier) + 16, "self-test state");
+    if (st != PC_OK) {
+        cudaStreamDestroy(s);
+        return st;
+    }
+    GridBarrier* gb = buf.as<GridBarrier>();
+    unsigned* tally = reinterpret_cast<unsigned*>(gb + 1);
+    unsigned* bad = tally + 1;
+    uint64_t limit_ns = (uint64_t)limit_ms * 1000000ull;
+    void* args[] = {(void*)&gb, (void*)&rounds, (void*)&absent_cta, (void*)&limit_ns, (void*)&tally, (void*)&bad};
+    GridBarrier hb{};
+    unsigned hbad = 0;
+    cudaError_t e = cudaMemsetAsync(buf.p, 0, sizeof(GridBarrier) + 16, s);
+    if (e == cudaSuccess)
+        e = cudaLaunchCooperativeKernel((const void*)k_grid_sync_selftest, dim3(grid), dim3(kThreads), args, 0, s);
+    count_launch();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hb, gb, sizeof(hb), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    if (e != cudaSuccess) return cuda_fail(e, "grid barrier self-test", __FILE__, __LINE__);
+    *mismatches = hbad;
+    if (hb.err) return fail(PC_ERR_TIMEOUT, "grid barrier: a wait ran out of time");
+    return PC_OK;
+}
+
 pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
     clear_error();
     if (!pg || !core_host) return fail(PC_ERR_INVALID_INPUT, "null argument");
@@ -597,7 +670,7 @@ pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
         if (largest) *largest = 0;
         return PC_OK;
     }
-    PC_TRY(scratch_reserve(pg, n * 4 * 7 + sizeof(KState) * 3));
+    PC_TRY(scratch_reserve(pg, n * 4 * 7 + sizeof(KState) * 3 + sizeof(GridBarrier) + 8));
     int32_t* deg = pg->scratch.take<int32_t>(n);
     int32_t* core = pg->scratch.take<int32_t>(n);
     int32_t* rem0 = pg->scratch.take<int32_t>(n);
@@ -606,7 +679,9 @@ pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
     int32_t* f1 = pg->scratch.take<int32_t>(n);
     int32_t* out = pg->scratch.take<int32_t>(n);
     KState* S = pg->scratch.take<KState>(3);
-    if (!S) return fail(PC_ERR_OOM, "k-core scratch plan exceeds its reservation");
+    GridBarrier* gb = pg->scratch.take<GridBarrier>(1);
+    uint64_t* d_steps = pg->scratch.take<uint64_t>(1);
+    if (!d_steps) return fail(PC_ERR_OOM, "k-core scratch plan exceeds its reservation");
     const unsigned nb = (unsigned)ceil_div(n, kThreads);
     k_kcore_init<<<nb, kThreads, 0, s>>>(pg->off, n, deg, core, rem0);
     PC_LAUNCHED();
@@ -616,31 +691,31 @@ pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
     // the minimum degree left, as the reference does (src/Graph.cpp:1921).
     // Vertices never peeled (only in a complete graph) keep core 0.
     KState init[3] = {};
-    init[0].k = 0;
-    init[0].fn = 0;
     init[0].rn = (uint32_t)n;
-    init[0].ml = 0;
-    init[0].phase = 0;
-    init[0].rpar = 0;
     init[1].ml = INT_MAX;
     PC_CUDA(cudaMemcpyAsync(S, init, sizeof(init), cudaMemcpyHostToDevice, s));
-    const unsigned grid = grid_for(pg, 8);
-    constexpr uint32_t kBatch = 32;
-    // every step either peels (shrinking the degrees) or advances the level,
-    // so n levels plus n peel rounds bound the steps
-    const uint64_t max_steps = 2 * n + 8;
-    uint32_t step = 0;
-    for (;;) {
-        for (uint32_t i = 0; i < kBatch; ++i, ++step) {
-            k_kcore_step<<<grid, kThreads, 0, s>>>(pg->off, pg->adj, n, deg, core, rem0, rem1, f0, f1, S, step);
-            PC_LAUNCHED();
-        }
-        int32_t done = 0;
-        PC_CUDA(cudaMemcpyAsync(&done, &S[step % 3].done, 4, cudaMemcpyDeviceToHost, s));
-        PC_CUDA(cudaStreamSynchronize(s));
-        if (done) break;
-        if (step > max_steps) return fail(PC_ERR_TIMEOUT, "k-core peeling did not finish");
-    }
+    PC_CUDA(cudaMemsetAsync(gb, 0, sizeof(GridBarrier), s));
+    int per_sm = 0;
+    PC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_kcore_persistent, kThreads, 0));
+    if (per_sm < 1) return fail(PC_ERR_CUDA, "k-core kernel cannot be resident");
+    const unsigned grid = (unsigned)(sm_count(pg->g->device) * std::min(per_sm, 4));
+    // every step either peels (lowering degrees) or advances the level, so n
+    // levels plus n peel rounds bound the steps
+    uint64_t max_steps = 2 * n + 8;
+    uint64_t limit_ns = kBarrierLimitNs;
+    const uint64_t* off = pg->off;
+    const int32_t* adj = pg->adj;
+    uint64_t nn = n;
+    void* args[] = {(void*)&off, (void*)&adj, (void*)&nn, (void*)&deg, (void*)&core, (void*)&rem0, (void*)&rem1,
+                    (void*)&f0, (void*)&f1, (void*)&S, (void*)&gb, (void*)&max_steps, (void*)&limit_ns,
+                    (void*)&d_steps};
+    PC_CUDA(cudaLaunchCooperativeKernel((const void*)k_kcore_persistent, dim3(grid), dim3(kThreads), args, 0, s));
+    PC_LAUNCHED();
+    GridBarrier hb{};
+    PC_CUDA(cudaMemcpyAsync(&hb, gb, sizeof(hb), cudaMemcpyDeviceToHost, s));
+    PC_CUDA(cudaStreamSynchronize(s));
+    if (hb.err == 1) return fail(PC_ERR_TIMEOUT, "k-core: a grid barrier wait ran out of time");
+    if (hb.err) return fail(PC_ERR_TIMEOUT, "k-core peeling did not finish within its step bound");
     k_kcore_unpeeled<<<nb, kThreads, 0, s>>>(core, n);
     PC_LAUNCHED();
     PC_TRY(gather_to_api_i32(pg, core, out));

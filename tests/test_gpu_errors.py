@@ -104,3 +104,23 @@ def test_rejects_bad_weights(gpu):
     assert "weights" in _raises_invalid(lambda: pc.Graph(vlist=vl, elist=el, weights=w)._device())
     w[0] = 1 << 30
     _raises_invalid(lambda: pc.Graph(vlist=vl, elist=el, weights=w)._device())
+
+
+def test_grid_barrier_is_bounded(gpu):
+    """The persistent kernels' grid barrier orders every CTA, and a CTA that
+    never arrives makes the others' waits run out (a short limit) into a
+    TIMEOUT status, leaving the device usable."""
+    pc = gpu
+    assert pc.selftest_grid_barrier(0, rounds=200) == 0
+    with pytest.raises(pc.PCError) as e:
+        pc.selftest_grid_barrier(0, rounds=4, absent_cta=3, limit_ms=100)
+    assert "ran out of time" in str(e.value)
+    assert pc.selftest_grid_barrier(0, rounds=8) == 0
+    h = pc.HostCSR.rmat(10, 8, 3)
+    vl, el, _ = h.arrays()
+    g = pc.Graph(vlist=vl, elist=el)
+    pg = pc.Partitioned_Graph(g, pc.equal_vertex_partition(vl.size - 1, 4))
+    from oracle import oracle as O
+    np.testing.assert_array_equal(pg.solve_kcore(), O.kcore(vl, el)[0])
+    pg.close()
+    g.close()

@@ -147,7 +147,15 @@ def test_lcc_and_jaccard(gpu, O, cases):
             np.testing.assert_array_equal(np.isnan(got), np.isnan(ref), err_msg=cid)
             np.testing.assert_array_equal(got, ref, err_msg=cid)
         if el.size:
-            np.testing.assert_array_equal(pg.jaccard_edges(), O.jaccard_edges(vl, el), err_msg=cid)
+            exp = O.jaccard_edges(vl, el)
+            np.testing.assert_array_equal(pg.jaccard_edges(), exp, err_msg=cid)
+            # caller-owned output (pinned host memory, as a pinned torch tensor gives)
+            import torch
+            pinned = torch.full((el.size,), -1.0, dtype=torch.float32, pin_memory=True).numpy()
+            assert pg.jaccard_edges(out=pinned) is pinned
+            np.testing.assert_array_equal(pinned, exp, err_msg=cid)
+            with pytest.raises(ValueError):
+                pg.jaccard_edges(out=np.empty(el.size + 1, np.float32))
         n = vl.size - 1
         if n:
             q = np.unique(np.random.default_rng(3).integers(0, n, min(n, 20))).astype(np.int32)
