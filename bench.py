@@ -600,27 +600,37 @@ def suite_algos(pc, O, args, emit):
     tc_bytes = tc_algorithmic_bytes(vl, el)[0]
     es_bytes = _edge_sum_bytes(vl, el)
     sweep = 4 * m + 8 * (n + 1) + 4 * n
+    import torch
+
+    def pinned(size, dt):
+        # caller-owned page-locked result buffer: the copy back runs at DMA speed
+        return torch.empty(size, dtype={np.int32: torch.int32, np.float32: torch.float32,
+                                        np.float64: torch.float64}[dt], pin_memory=True).numpy()
+
+    o_lcc, o_jac = pinned(n, np.float64), pinned(m, np.float32)
+    o_bfs, o_sssp, o_pr, o_pr64 = pinned(n, np.int32), pinned(n, np.int32), pinned(n, np.float32), pinned(n, np.float64)
+    o_kc, o_mis, o_mish, o_cd = pinned(n, np.int32), pinned(n, np.int32), pinned(n, np.int32), pinned(n, np.int32)
     cases = [
         # name, gpu call, cpu (kind, call), units, bytes, compare
         # the reference's own TC and LCC loops take minutes here (static OpenMP schedule over
         # degree-sorted rows: 91 s for TC on 16 cores); the oracle (dynamic schedule) checks them
         ("tc", lambda: pg.triangle_count(), ("port", lambda: O.tc_merge(vl, el)), m // 2, tc_bytes, "exact"),
         ("tc_galloping", lambda: pg.solve_triangle_counting_galloping(), None, m // 2, tc_bytes, "exact6"),
-        ("lcc", lambda: pg.solve_lcc_merge(), ("port", lambda: O.lcc(vl, el)), m, es_bytes, 1e-6),
-        ("jaccard_edges", lambda: pg.jaccard_edges(), ("port", lambda: O.jaccard_edges(vl, el)), m, es_bytes, 1e-6),
-        ("bfs", lambda: pg.solve_bfs(0), ("port", lambda: O.bfs(vl, el, 0)), m, sweep, "exact"),
-        ("sssp", lambda: pg.solve_sssp(0), ("port", lambda: O.sssp(vl, el, w, 0)), m, sweep, "exact"),
-        ("pagerank_fp32", lambda: pg.page_rank(0.85, 20), ("port", lambda: O.pagerank_f64(vl, el, 0.85, 20)),
+        ("lcc", lambda: pg.solve_lcc_merge(out=o_lcc), ("port", lambda: O.lcc(vl, el)), m, es_bytes, 1e-6),
+        ("jaccard_edges", lambda: pg.jaccard_edges(out=o_jac), ("port", lambda: O.jaccard_edges(vl, el)), m, es_bytes, 1e-6),
+        ("bfs", lambda: pg.solve_bfs(0, out=o_bfs), ("port", lambda: O.bfs(vl, el, 0)), m, sweep, "exact"),
+        ("sssp", lambda: pg.solve_sssp(0, out=o_sssp), ("port", lambda: O.sssp(vl, el, w, 0)), m, sweep, "exact"),
+        ("pagerank_fp32", lambda: pg.page_rank(0.85, 20, out=o_pr), ("port", lambda: O.pagerank_f64(vl, el, 0.85, 20)),
          m * 20, 20 * (8 * m + 20 * n), 1e-6),
-        ("pagerank_fp64", lambda: pg.page_rank(0.85, 20, fp64=True),
+        ("pagerank_fp64", lambda: pg.page_rank(0.85, 20, fp64=True, out=o_pr64),
          ("port", lambda: O.pagerank_f64(vl, el, 0.85, 20)), m * 20, 20 * (12 * m + 24 * n), 1e-12),
-        ("kcore", lambda: pg.solve_kcore(), ("reference", lambda: R.kcore()) if R else ("port", lambda: O.kcore(vl, el)),
+        ("kcore", lambda: pg.solve_kcore(out=o_kc), ("reference", lambda: R.kcore()) if R else ("port", lambda: O.kcore(vl, el)),
          m, sweep, "exact"),
-        ("mis", lambda: pg.solve_mis(), ("reference", lambda: R.mis()) if R else ("port", lambda: O.mis(vl, el)),
+        ("mis", lambda: pg.solve_mis(out=o_mis), ("reference", lambda: R.mis()) if R else ("port", lambda: O.mis(vl, el)),
          m, sweep, "exact"),
-        ("mis_hashed", lambda: pg.solve_mis(seed=args.seed), ("port", lambda: O.mis(vl, el, priority=prio)),
+        ("mis_hashed", lambda: pg.solve_mis(seed=args.seed, out=o_mish), ("port", lambda: O.mis(vl, el, priority=prio)),
          m, sweep, "exact"),
-        ("cdlp", lambda: pg.solve_cdlp(lab0, 10),
+        ("cdlp", lambda: pg.solve_cdlp(lab0, 10, out=o_cd),
          ("reference", lambda: R.cdlp(lab0, 10)) if R else ("port", lambda: O.cdlp(vl, el, lab0, 10)),
          m * 10, 10 * sweep, "exact"),
     ]
@@ -631,6 +641,8 @@ def suite_algos(pc, O, args, emit):
                "m_directed": int(m), "gpu_ms": round(t_gpu * 1e3, 3), "gteps": round(units / t_gpu / 1e9, 4),
                "algorithmic_gbs": round(nbytes / t_gpu / 1e9, 1), "hbm_frac": round(nbytes / t_gpu / 1e9 / peak, 4),
                "peak_kind": peak_kind}
+        if isinstance(out, np.ndarray):
+            rec["result_buffer"] = "caller-owned pinned host array"
         if cpu is None:
             ok, err = (int(out) == 6 * ref_tc), 0.0
             rec.update({"parity": "exact (6 T)" if ok else "MISMATCH"})

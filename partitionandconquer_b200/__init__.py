@@ -54,6 +54,20 @@ def vertex_priority(seed: int, n: int) -> np.ndarray:
     return out
 
 
+def _result(out, size: int, dtype) -> np.ndarray:
+    """The array a call writes its result into: a new one, or the caller's
+    `out`, which must be a writeable C-contiguous array of `size` entries of
+    `dtype`.  Page-locked memory (a pinned torch tensor's .numpy(), or an
+    array registered with pc_host_register) lets the copy back run at DMA
+    speed; a new pageable array is faulted in by the copy itself."""
+    if out is None:
+        return np.empty(size, dtype)
+    if (not isinstance(out, np.ndarray) or out.dtype != np.dtype(dtype) or out.size != size
+            or not out.flags.c_contiguous or not out.flags.writeable):
+        raise ValueError(f"out must be a writeable C-contiguous {np.dtype(dtype).name} array of {size} entries")
+    return out
+
+
 def equal_vertex_partition(n: int, P: int) -> np.ndarray:
     """part(u) = floor(u * P / n): P contiguous blocks of equal vertex count."""
     return ((np.arange(n, dtype=np.int64) * P) // max(n, 1)).astype(np.int32)
@@ -67,7 +81,7 @@ class HostCSR:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and lib is not None:  # at interpreter exit the module may be torn down first
             lib.pc_host_csr_free(h)
             self._h = None
 
@@ -440,28 +454,23 @@ class Partitioned_Graph:
     def solve_triangle_counting_galloping(self) -> int:
         return self.triangle_count(METHOD_GALLOPING)
 
-    def _lcc(self, method):
-        out = np.empty(self.get_vertex_num(), np.float64)
+    def _lcc(self, method, out):
+        out = _result(out, self.get_vertex_num(), np.float64)
         check(lib.pc_lcc(self._pg, method, ptr(out)))
         return out
 
-    def solve_lcc_merge(self):
-        return self._lcc(METHOD_MERGE)
+    def solve_lcc_merge(self, out=None):
+        return self._lcc(METHOD_MERGE, out)
 
-    def solve_lcc_galloping(self):
-        return self._lcc(METHOD_GALLOPING)
+    def solve_lcc_galloping(self, out=None):
+        return self._lcc(METHOD_GALLOPING, out)
 
     def jaccard_edges(self, out=None):
         """J per CSR entry (fp32).  `out`, when given, is a C-contiguous float32
         host array of get_edge_num() entries that receives the values; pinned
         memory (e.g. a pinned torch tensor's .numpy()) makes the copy back run
         at DMA speed instead of being staged through the driver."""
-        m = self.get_edge_num()
-        if out is None:
-            out = np.empty(m, np.float32)
-        elif (not isinstance(out, np.ndarray) or out.dtype != np.float32 or out.size != m
-              or not out.flags.c_contiguous or not out.flags.writeable):
-            raise ValueError(f"out must be a writeable C-contiguous float32 array of {m} entries")
+        out = _result(out, self.get_edge_num(), np.float32)
         check(lib.pc_jaccard_edges(self._pg, ptr(out)))
         return out
 
@@ -516,46 +525,54 @@ class Partitioned_Graph:
     batch_cnt_common_neis_galloping_fine_grained = batch_cnt_common_neis_merge
 
     # -- frontier algorithms --
-    def solve_bfs(self, u: int):
-        out = np.empty(self.get_vertex_num(), np.int32)
+    # Every method below takes an optional `out`: a caller-owned host array
+    # of the result's size and dtype that receives the result (see _result).
+    def solve_bfs(self, u: int, out=None):
+        out = _result(out, self.get_vertex_num(), np.int32)
         check(lib.pc_bfs(self._pg, u, ptr(out)))
         return out
 
-    def solve_sssp(self, src: int):
-        out = np.empty(self.get_vertex_num(), np.int32)
+    def solve_sssp(self, src: int, out=None):
+        out = _result(out, self.get_vertex_num(), np.int32)
         check(lib.pc_sssp(self._pg, src, ptr(out)))
         return out
 
-    def page_rank(self, damping_factor: float = 0.85, num_iterations: int = 20, init=None, fp64: bool = False):
+    def page_rank(self, damping_factor: float = 0.85, num_iterations: int = 20, init=None, fp64: bool = False,
+                  out=None):
         n = self.get_vertex_num()
         if fp64:
-            out = np.empty(n, np.float64)
+            out = _result(out, n, np.float64)
             ini = None if init is None else _lib.as_array(init, np.float64)
             check(lib.pc_pagerank_f64(self._pg, float(damping_factor), num_iterations, ptr(ini), ptr(out)))
         else:
-            out = np.empty(n, np.float32)
+            out = _result(out, n, np.float32)
             ini = None if init is None else _lib.as_array(init, np.float32)
             check(lib.pc_pagerank(self._pg, float(damping_factor), num_iterations, ptr(ini), ptr(out)))
         return out
 
-    def solve_kcore(self):
-        out = np.empty(self.get_vertex_num(), np.int32)
+    def solve_kcore(self, out=None):
+        out = _result(out, self.get_vertex_num(), np.int32)
         largest = C.c_int32()
         check(lib.pc_kcore(self._pg, ptr(out), C.byref(largest)))
         return out
 
-    def solve_mis(self, seed: Optional[int] = None):
-        out = np.empty(self.get_vertex_num(), np.int32)
+    def solve_mis(self, seed: Optional[int] = None, out=None):
+        out = _result(out, self.get_vertex_num(), np.int32)
         if seed is None:
             check(lib.pc_mis(self._pg, ptr(out)))
         else:
             check(lib.pc_mis_hashed(self._pg, seed, ptr(out)))
         return out
 
-    def solve_cdlp(self, labels, max_iterations: int):
-        lab = _lib.as_array(labels, np.int32).copy()
-        check(lib.pc_cdlp(self._pg, max_iterations, ptr(lab)))
-        return lab
+    def solve_cdlp(self, labels, max_iterations: int, out=None):
+        """Labels are updated in a copy (or in `out`); the input stays as it was."""
+        lab = _lib.as_array(labels, np.int32)
+        out = _result(out, self.get_vertex_num(), np.int32)
+        if lab.size != out.size:
+            raise ValueError(f"labels must have {out.size} entries")
+        out[:] = lab
+        check(lib.pc_cdlp(self._pg, max_iterations, ptr(out)))
+        return out
 
 
 class Batch:

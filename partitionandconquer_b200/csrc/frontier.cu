@@ -9,6 +9,8 @@
 #include <cmath>
 #include <vector>
 
+#include <cub/block/block_scan.cuh>
+
 #include "grid_sync.cuh"
 #include "pc_internal.cuh"
 #include "synth_rng.h"
@@ -20,6 +22,9 @@ constexpr int kThreads = 256;
 constexpr int32_t kInf = INT_MAX;
 // bound on any grid-barrier wait of the persistent kernels (4 s)
 constexpr uint64_t kBarrierLimitNs = 4000000000ull;
+// k-core: ids below this have their degree decrements gathered per CTA
+constexpr int kKcoreHubs = 4096;
+static_assert(kKcoreHubs % kThreads == 0, "the flush loop needs a uniform trip count");
 
 // Appends `val` for every lane with pred set; all 32 lanes of the warp must
 // call it together.
@@ -39,6 +44,72 @@ __device__ __forceinline__ uint64_t warp_sum_u64(uint64_t x) {
     return x;
 }
 
+// ---- rows longer than kHeavyDeg ------------------------------------------------
+// A warp-per-vertex loop serialises a hub's row on one warp (RMAT-22's largest
+// row has 163K entries: 5100 rounds of dependent loads on one warp).  The
+// frontier kernels set such vertices aside in a heavy list; heavy_rows() then
+// spreads the rows of the list over every warp of the grid in chunks of
+// kHeavyChunk entries, balanced by a block-local prefix of chunk counts.
+constexpr uint32_t kHeavyDeg = 1024;
+constexpr uint32_t kHeavyChunk = 256;
+constexpr uint32_t kHeavyBatch = 2048;  // list entries per shared-memory prefix
+static_assert(kHeavyBatch % kThreads == 0, "prefix items per thread");
+
+// Calls body(u, j, valid) for the entries j of every row of hq[0..hn); the 32
+// lanes of a warp call it together (valid is false past a row's end), so the
+// body may use warp collectives.  All threads of every CTA must call it.
+template <class Body>
+__device__ __forceinline__ void heavy_rows(const uint64_t* __restrict__ off, const int32_t* hq, uint32_t hn,
+                                           Body&& body) {
+    using Scan = cub::BlockScan<uint32_t, kThreads>;
+    __shared__ typename Scan::TempStorage scan_tmp;
+    __shared__ uint32_t s_pref[kHeavyBatch + 1];
+    constexpr int kPer = kHeavyBatch / kThreads;
+    const int lane = threadIdx.x & 31;
+    const uint64_t wpb = blockDim.x >> 5;
+    const uint64_t gw = blockIdx.x * wpb + (threadIdx.x >> 5), nw = (uint64_t)gridDim.x * wpb;
+    for (uint32_t h0 = 0; h0 < hn; h0 += kHeavyBatch) {
+        const uint32_t hb = min(kHeavyBatch, hn - h0);
+        uint32_t cnt[kPer];
+        for (int t = 0; t < kPer; ++t) {
+            const uint32_t h = threadIdx.x * kPer + t;
+            cnt[t] = 0;
+            if (h < hb) {
+                const int32_t u = __ldcg(hq + h0 + h);
+                cnt[t] = (uint32_t)((off[u + 1] - off[u] + kHeavyChunk - 1) / kHeavyChunk);
+            }
+        }
+        __syncthreads();  // the previous batch is done with s_pref and scan_tmp
+        uint32_t total = 0;
+        Scan(scan_tmp).ExclusiveSum(cnt, cnt, total);
+        for (int t = 0; t < kPer; ++t) s_pref[threadIdx.x * kPer + t] = cnt[t];
+        if (threadIdx.x == 0) s_pref[kHeavyBatch] = total;
+        __syncthreads();
+        for (uint64_t c = gw; c < total; c += nw) {
+            uint32_t lo = 0, hi = hb - 1;  // last row whose chunks start at or before c
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (s_pref[mid] <= c) lo = mid; else hi = mid - 1;
+            }
+            const int32_t u = __ldcg(hq + h0 + lo);
+            const uint64_t rb = off[u] + (c - s_pref[lo]) * (uint64_t)kHeavyChunk;
+            const uint64_t re = min(rb + kHeavyChunk, off[u + 1]);
+            for (uint64_t j0 = rb; j0 < re; j0 += 32) body(u, j0 + lane, j0 + lane < re);
+        }
+    }
+}
+
+// Rows of more than kHeavyDeg entries (pull kernels give each a whole CTA).
+__global__ void k_heavy_list(const uint64_t* __restrict__ off, uint64_t n, int32_t* __restrict__ hq,
+                             uint32_t* __restrict__ hn) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t nr = (n + 31) & ~31ull;
+    for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < nr; u += stride) {
+        const bool heavy = u < n && off[u + 1] - off[u] > kHeavyDeg;
+        warp_append(heavy, (int32_t)u, hq, hn);
+    }
+}
+
 // ---- BFS -------------------------------------------------------------------
 
 __global__ void k_iota(int32_t* a, uint64_t n) {
@@ -55,7 +126,8 @@ __global__ void k_fill_i32(int32_t* a, uint64_t n, int32_t v) {
 __global__ void k_bfs_top_down(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
                                const int32_t* __restrict__ fq, uint32_t fn, int32_t* __restrict__ dist,
                                int32_t level, int32_t* __restrict__ nq, uint32_t* __restrict__ nn,
-                               unsigned long long* __restrict__ next_edges) {
+                               unsigned long long* __restrict__ next_edges, int32_t* __restrict__ hq,
+                               uint32_t* __restrict__ hn) {
     const int lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -63,6 +135,10 @@ __global__ void k_bfs_top_down(const uint64_t* __restrict__ off, const int32_t* 
     for (uint64_t i = warp; i < fn; i += nwarps) {
         const int32_t u = fq[i];
         const uint64_t b = off[u], e = off[u + 1];
+        if (e - b > kHeavyDeg) {  // expanded by k_bfs_top_down_heavy
+            if (lane == 0) hq[atomicAdd(hn, 1u)] = u;
+            continue;
+        }
         for (uint64_t j0 = b; j0 < e; j0 += 32) {
             const uint64_t j = j0 + lane;
             bool won = false;
@@ -77,6 +153,26 @@ __global__ void k_bfs_top_down(const uint64_t* __restrict__ off, const int32_t* 
     }
     edges = warp_sum_u64(edges);
     if (lane == 0 && edges) atomicAdd(next_edges, (unsigned long long)edges);
+}
+
+// The heavy frontier vertices of a top-down step, spread over the grid.
+__global__ void k_bfs_top_down_heavy(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                                     const int32_t* __restrict__ hq, const uint32_t* __restrict__ hn,
+                                     int32_t* __restrict__ dist, int32_t level, int32_t* __restrict__ nq,
+                                     uint32_t* __restrict__ nn, unsigned long long* __restrict__ next_edges) {
+    uint64_t edges = 0;
+    heavy_rows(off, hq, *hn, [&](int32_t, uint64_t j, bool ok) {
+        bool won = false;
+        int32_t v = 0;
+        if (ok) {
+            v = adj[j];
+            if (dist[v] == kInf) won = atomicCAS(&dist[v], kInf, level) == kInf;
+        }
+        if (won) edges += off[v + 1] - off[v];
+        warp_append(won, v, nq, nn);
+    });
+    edges = warp_sum_u64(edges);
+    if ((threadIdx.x & 31) == 0 && edges) atomicAdd(next_edges, (unsigned long long)edges);
 }
 
 // Bottom-up step: every unvisited vertex looks for a neighbour at level-1.
@@ -114,14 +210,18 @@ __global__ void k_bfs_finish(const int32_t* __restrict__ dist, uint64_t n, int32
 __global__ void k_sssp_relax(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
                              const int32_t* __restrict__ w, const int32_t* __restrict__ fq, uint32_t fn,
                              int32_t* __restrict__ dist, int32_t* __restrict__ flag, int32_t* __restrict__ nq,
-                             uint32_t* __restrict__ nn) {
+                             uint32_t* __restrict__ nn, int32_t* __restrict__ hq, uint32_t* __restrict__ hn) {
     const int lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = warp; i < fn; i += nwarps) {
         const int32_t u = fq[i];
-        const int32_t du = dist[u];
         const uint64_t b = off[u], e = off[u + 1];
+        if (e - b > kHeavyDeg) {  // relaxed by k_sssp_relax_heavy
+            if (lane == 0) hq[atomicAdd(hn, 1u)] = u;
+            continue;
+        }
+        const int32_t du = dist[u];
         for (uint64_t j0 = b; j0 < e; j0 += 32) {
             const uint64_t j = j0 + lane;
             bool push = false;
@@ -137,6 +237,28 @@ __global__ void k_sssp_relax(const uint64_t* __restrict__ off, const int32_t* __
             warp_append(push, v, nq, nn);
         }
     }
+}
+
+// The heavy frontier vertices of a relaxation round, spread over the grid.
+// dist[u] may fall further while its row is being relaxed; any value read is
+// an achieved distance, and a vertex whose distance falls is queued again.
+__global__ void k_sssp_relax_heavy(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                                   const int32_t* __restrict__ w, const int32_t* __restrict__ hq,
+                                   const uint32_t* __restrict__ hn, int32_t* __restrict__ dist,
+                                   int32_t* __restrict__ flag, int32_t* __restrict__ nq, uint32_t* __restrict__ nn) {
+    heavy_rows(off, hq, *hn, [&](int32_t u, uint64_t j, bool ok) {
+        bool push = false;
+        int32_t v = 0;
+        if (ok) {
+            v = adj[j];
+            const int32_t nd = dist[u] + w[j];
+            if (nd < dist[v]) {
+                const int32_t old = atomicMin(&dist[v], nd);
+                if (nd < old) push = atomicExch(&flag[v], 1) == 0;
+            }
+        }
+        warp_append(push, v, nq, nn);
+    });
 }
 
 __global__ void k_clear_flags(const int32_t* __restrict__ q, uint32_t qn, int32_t* __restrict__ flag) {
@@ -164,23 +286,53 @@ __global__ void k_pr_init(const uint64_t* __restrict__ off, uint64_t n, T dampin
 // storage rounding (within 1e-6 relative of the FP64 recurrence at 20
 // iterations; fp32 row sums over hub in-lists drift past that).
 template <class T>
-__global__ void k_pr_iter(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj, uint64_t n, double base,
-                          const T* __restrict__ degs, const T* __restrict__ contrib, T* __restrict__ x_out,
-                          T* __restrict__ contrib_out) {
-    const int lane = threadIdx.x & 31;
+__device__ __forceinline__ void pr_epilogue(uint64_t v, double base, double sum, const T* __restrict__ degs,
+                                            T* __restrict__ x_out, T* __restrict__ contrib_out) {
+    const double x = base + sum;
+    x_out[v] = (T)x;
+    const double dg = (double)degs[v];
+    contrib_out[v] = dg > 0.0 ? (T)(x / dg) : (T)0;
+}
+
+// One iteration: x'[v] = base + sum_{u in N(v)} contrib[u]; contrib'[v] = x'[v] / degs[v].
+// T is the storage type of the vectors; the row sums, x' and the division
+// run in fp64 for both instances, so the fp32 vectors carry only their own
+// storage rounding (within 1e-6 relative of the FP64 recurrence at 20
+// iterations; fp32 row sums over hub in-lists drift past that).  Rows listed
+// in hq (more than kHeavyDeg entries) get a whole CTA each; the others a
+// warp.  Both reductions run in a fixed order, so results are reproducible.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_pr_iter(const uint64_t* __restrict__ off,
+                                                      const int32_t* __restrict__ adj, uint64_t n, double base,
+                                                      const T* __restrict__ degs, const T* __restrict__ contrib,
+                                                      T* __restrict__ x_out, T* __restrict__ contrib_out,
+                                                      const int32_t* __restrict__ hq, uint32_t hn) {
+    __shared__ double s_part[kThreads / 32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    for (uint32_t h = blockIdx.x; h < hn; h += gridDim.x) {
+        const int32_t v = hq[h];
+        const uint64_t b = off[v], e = off[v + 1];
+        double s = 0.0;
+        for (uint64_t j = b + threadIdx.x; j < e; j += kThreads) s += (double)__ldg(contrib + adj[j]);
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) s_part[wib] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int i = 0; i < kThreads / 32; ++i) t += s_part[i];
+            pr_epilogue(v, base, t, degs, x_out, contrib_out);
+        }
+        __syncthreads();
+    }
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t v = warp; v < n; v += nwarps) {
         const uint64_t b = off[v], e = off[v + 1];
+        if (e - b > kHeavyDeg) continue;
         double s = 0.0;
         for (uint64_t j = b + lane; j < e; j += 32) s += (double)__ldg(contrib + adj[j]);
         for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) {
-            const double x = base + s;
-            x_out[v] = (T)x;
-            const double dg = (double)degs[v];
-            contrib_out[v] = dg > 0.0 ? (T)(x / dg) : (T)0;
-        }
+        if (lane == 0) pr_epilogue(v, base, s, degs, x_out, contrib_out);
     }
 }
 
@@ -201,7 +353,10 @@ __global__ void k_kcore_init(const uint64_t* __restrict__ off, uint64_t n, int32
 // rotating records: step i reads S[i % 3], accumulates into S[(i+1) % 3]
 // (counters cleared by step i-1) and clears S[(i+2) % 3], which no CTA reads
 // during step i.  Mutable arrays are read with __ldcg: L1 is not coherent
-// across CTAs within one launch.
+// across CTAs within one launch.  Frontier vertices with more than kHeavyDeg
+// neighbours are set aside (hq0/hq1 by step parity) and their rows are peeled
+// in the next step, spread over the grid; that step is still a peel round of
+// the same level, so every decrement of a level lands before its next scan.
 struct KState {
     int32_t k;      // level of the step that wrote this record
     uint32_t fn;    // frontier size it produced
@@ -210,7 +365,7 @@ struct KState {
     int32_t phase;  // 0 scan, 1 peel
     int32_t fpar;   // frontier buffer holding the frontier
     int32_t rpar;   // remaining-list buffer
-    int32_t pad;
+    uint32_t hn;    // heavy frontier vertices it set aside for the next step
 };
 
 __device__ __forceinline__ KState load_state(const KState* p) {
@@ -224,14 +379,21 @@ __device__ __forceinline__ KState load_state(const KState* p) {
     s.phase = hi.x;
     s.fpar = hi.y;
     s.rpar = hi.z;
-    s.pad = hi.w;
+    s.hn = (uint32_t)hi.w;
     return s;
 }
 
 __global__ void __launch_bounds__(kThreads) k_kcore_persistent(
     const uint64_t* __restrict__ off, const int32_t* __restrict__ adj, uint64_t n, int32_t* deg, int32_t* core,
-    int32_t* rem0, int32_t* rem1, int32_t* f0, int32_t* f1, KState* S, GridBarrier* gb, uint64_t max_steps,
-    uint64_t limit_ns, uint64_t* steps_done) {
+    int32_t* rem0, int32_t* rem1, int32_t* f0, int32_t* f1, int32_t* hq0, int32_t* hq1, KState* S,
+    GridBarrier* gb, uint64_t max_steps, uint64_t limit_ns, uint64_t* steps_done) {
+    // decrements of the lowest ids (the hubs, once ids are degree-ordered)
+    // are gathered per CTA in shared memory and applied once per step
+    __shared__ int32_t s_dec[kKcoreHubs];
+    __shared__ int s_any;
+    for (int i = threadIdx.x; i < kKcoreHubs; i += blockDim.x) s_dec[i] = 0;
+    if (threadIdx.x == 0) s_any = 0;
+    __syncthreads();
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
     const int lane = threadIdx.x & 31;
     const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -241,7 +403,7 @@ __global__ void __launch_bounds__(kThreads) k_kcore_persistent(
     for (; step < max_steps; ++step) {
         const KState in = load_state(&S[step % 3]);
         KState* out = &S[(step + 1) % 3];
-        const bool peel = in.fn > 0;
+        const bool peel = in.fn > 0 || in.hn > 0;
         const int32_t k = peel ? in.k
                                : ((in.phase == 1 || in.ml == INT_MAX) ? in.k + 1 : max(in.k + 1, in.ml + 1));
         // every CTA reads the same record, so all leave at the same step
@@ -251,6 +413,7 @@ __global__ void __launch_bounds__(kThreads) k_kcore_persistent(
             clr->fn = 0;
             clr->rn = 0;
             clr->ml = INT_MAX;
+            clr->hn = 0;
             if (peel) out->rn = in.rn;  // a peel round keeps the remaining list
             out->k = k;
             out->phase = peel ? 1 : 0;
@@ -260,16 +423,19 @@ __global__ void __launch_bounds__(kThreads) k_kcore_persistent(
         if (peel) {
             const int32_t* fq = in.fpar ? f1 : f0;
             int32_t* nq = in.fpar ? f0 : f1;
-            for (uint64_t i = warp; i < in.fn; i += nwarps) {
-                const int32_t u = __ldcg(fq + i);
-                const uint64_t b = off[u], e = off[u + 1];
-                for (uint64_t j0 = b; j0 < e; j0 += 32) {
-                    const uint64_t j = j0 + lane;
-                    bool push = false;
-                    int32_t v = 0;
-                    if (j < e) {
-                        v = adj[j];
-                        if (__ldcg(core + v) < 0) {
+            int32_t* hq_next = (step & 1) ? hq1 : hq0;
+            const int32_t* hq_prev = (step & 1) ? hq0 : hq1;
+            // one CSR entry (u, v) of a peeled vertex u; all lanes call it
+            auto peel_entry = [&](uint64_t j, bool ok) {
+                bool push = false;
+                int32_t v = 0;
+                if (ok) {
+                    v = adj[j];
+                    if (__ldcg(core + v) < 0) {
+                        if (v < kKcoreHubs) {
+                            atomicAdd(&s_dec[v], 1);
+                            s_any = 1;
+                        } else {
                             const int32_t old = atomicSub(&deg[v], 1);
                             if (old == k) {
                                 push = true;
@@ -277,8 +443,38 @@ __global__ void __launch_bounds__(kThreads) k_kcore_persistent(
                             }
                         }
                     }
-                    warp_append(push, v, nq, &out->fn);
                 }
+                warp_append(push, v, nq, &out->fn);
+            };
+            for (uint64_t i = warp; i < in.fn; i += nwarps) {
+                const int32_t u = __ldcg(fq + i);
+                const uint64_t b = off[u], e = off[u + 1];
+                if (e - b > kHeavyDeg) {
+                    if (lane == 0) hq_next[atomicAdd(&out->hn, 1u)] = u;
+                    continue;
+                }
+                for (uint64_t j0 = b; j0 < e; j0 += 32) peel_entry(j0 + lane, j0 + lane < e);
+            }
+            heavy_rows(off, hq_prev, in.hn, [&](int32_t, uint64_t j, bool ok) { peel_entry(j, ok); });
+            // flush the gathered hub decrements: the one flush that takes a
+            // degree from >= k to < k pushes the vertex
+            __syncthreads();
+            if (s_any) {
+                for (int i = threadIdx.x; i < kKcoreHubs; i += blockDim.x) {
+                    const int32_t c = s_dec[i];
+                    bool push = false;
+                    if (c) {
+                        s_dec[i] = 0;
+                        const int32_t old = atomicSub(&deg[i], c);
+                        if (old >= k && old - c < k) {
+                            push = true;
+                            core[i] = k - 1;
+                        }
+                    }
+                    warp_append(push, i, nq, &out->fn);
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) s_any = 0;
             }
         } else {
             // scan of level k over the remaining list
@@ -343,15 +539,19 @@ __global__ void k_kcore_unpeeled(int32_t* __restrict__ core, uint64_t n) {
 // are final and only made from final neighbour states, so the in-place update
 // reaches the unique greedy (lexicographically-first) set.
 __global__ void k_mis_round(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
-                            const uint64_t* __restrict__ prio, const int32_t* __restrict__ uq, uint32_t un,
-                            int32_t* __restrict__ state, int32_t* __restrict__ nq, uint32_t* __restrict__ nn) {
+                            const uint64_t* __restrict__ prio, const uint32_t* __restrict__ dplus,
+                            const int32_t* __restrict__ uq, uint32_t un, int32_t* __restrict__ state,
+                            int32_t* __restrict__ nq, uint32_t* __restrict__ nn) {
     const int lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = warp; i < un; i += nwarps) {
         const int32_t u = uq[i];
         const uint64_t pu = prio ? prio[u] : (uint64_t)u;
-        const uint64_t b = off[u], e = off[u + 1];
+        // with id priorities only the neighbours below u matter: an IN
+        // neighbour v > u would need u OUT first, and only v < u block
+        // (rows are sorted, so those are the first dplus[u] entries)
+        const uint64_t b = off[u], e = dplus ? b + dplus[u] : off[u + 1];
         bool in_nbr = false, blocked = false;
         for (uint64_t j0 = b; j0 < e; j0 += 32) {
             const uint64_t j = j0 + lane;
@@ -391,14 +591,36 @@ __global__ void k_mis_finish(const int32_t* __restrict__ state, uint64_t n, int3
 
 // ---- CDLP --------------------------------------------------------------------------
 
-__global__ void k_cdlp_iter(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj, uint64_t n,
-                            const int32_t* __restrict__ lab, int32_t* __restrict__ out) {
-    const int lane = threadIdx.x & 31;
+// One iteration: out[v] = max label over N(v), 0 for an isolated vertex
+// (src/Graph.cpp:650: labels start at 0 for every vertex).  Rows listed in hq
+// get a whole CTA each; the others a warp.
+__global__ void __launch_bounds__(kThreads) k_cdlp_iter(const uint64_t* __restrict__ off,
+                                                        const int32_t* __restrict__ adj, uint64_t n,
+                                                        const int32_t* __restrict__ lab, int32_t* __restrict__ out,
+                                                        const int32_t* __restrict__ hq, uint32_t hn) {
+    __shared__ int32_t s_part[kThreads / 32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    for (uint32_t h = blockIdx.x; h < hn; h += gridDim.x) {
+        const int32_t v = hq[h];
+        const uint64_t b = off[v], e = off[v + 1];
+        int32_t mx = 0;
+        for (uint64_t j = b + threadIdx.x; j < e; j += kThreads) mx = max(mx, __ldg(lab + adj[j]));
+        for (int o = 16; o; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0) s_part[wib] = mx;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int32_t t = 0;
+            for (int i = 0; i < kThreads / 32; ++i) t = max(t, s_part[i]);
+            out[v] = t;
+        }
+        __syncthreads();
+    }
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t v = warp; v < n; v += nwarps) {
         const uint64_t b = off[v], e = off[v + 1];
-        int32_t mx = 0;  // src/Graph.cpp:650: labels start at 0 for every vertex
+        if (e - b > kHeavyDeg) continue;
+        int32_t mx = 0;
         for (uint64_t j = b + lane; j < e; j += 32) mx = max(mx, __ldg(lab + adj[j]));
         for (int o = 16; o; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
         if (lane == 0) out[v] = mx;
@@ -411,6 +633,22 @@ using namespace fr;
 
 static unsigned grid_for(const pc_pgraph* pg, int per_sm = 8) { return (unsigned)(sm_count(pg->g->device) * per_sm); }
 
+// Entries a heavy list can need: rows of more than kHeavyDeg entries.
+static uint64_t heavy_cap(uint64_t n, uint64_t m) { return std::max<uint64_t>(1, std::min<uint64_t>(n, m / kHeavyDeg + 1)); }
+
+// Lists the rows of more than kHeavyDeg entries into hq (room for heavy_cap
+// entries) and reads their number back.
+static pc_status list_heavy_rows(pc_pgraph* pg, int32_t* hq, uint32_t* d_hn, uint32_t* hn) {
+    if (!hq || !d_hn) return fail(PC_ERR_OOM, "scratch plan exceeds its reservation");
+    cudaStream_t s = pg->g->stream;
+    PC_CUDA(cudaMemsetAsync(d_hn, 0, 4, s));
+    k_heavy_list<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->g->n, hq, d_hn);
+    PC_LAUNCHED();
+    PC_CUDA(cudaMemcpyAsync(hn, d_hn, 4, cudaMemcpyDeviceToHost, s));
+    PC_CUDA(cudaStreamSynchronize(s));
+    return PC_OK;
+}
+
 // Reads a device counter (synchronising the stream).
 static pc_status read_u32(pc_pgraph* pg, const uint32_t* d, uint32_t* h) {
     PC_CUDA(cudaMemcpyAsync(h, d, 4, cudaMemcpyDeviceToHost, pg->g->stream));
@@ -421,12 +659,15 @@ static pc_status read_u32(pc_pgraph* pg, const uint32_t* d, uint32_t* h) {
 static pc_status bfs_run(pc_pgraph* pg, int32_t src, int32_t* rank_host) {
     const uint64_t n = pg->g->n, m = pg->g->m;
     cudaStream_t s = pg->g->stream;
-    PC_TRY(scratch_reserve(pg, n * 4 * 4 + 256));
+    const uint64_t hcap = heavy_cap(n, m);
+    PC_TRY(scratch_reserve(pg, n * 4 * 4 + hcap * 4 + 256));
     int32_t* dist = pg->scratch.take<int32_t>(n);
     int32_t* q0 = pg->scratch.take<int32_t>(n);
     int32_t* q1 = pg->scratch.take<int32_t>(n);
-    uint32_t* cnt = pg->scratch.take<uint32_t>(4);
+    int32_t* hq = pg->scratch.take<int32_t>(hcap);
+    uint32_t* cnt = pg->scratch.take<uint32_t>(4);  // [0] next frontier, [1] heavy list
     unsigned long long* edges = pg->scratch.take<unsigned long long>(2);
+    if (!edges) return fail(PC_ERR_OOM, "BFS scratch plan exceeds its reservation");
     const unsigned nb = (unsigned)ceil_div(n, kThreads);
     k_fill_i32<<<nb, kThreads, 0, s>>>(dist, n, kInf);
     PC_LAUNCHED();
@@ -447,12 +688,16 @@ static pc_status bfs_run(pc_pgraph* pg, int32_t src, int32_t* rank_host) {
     for (int32_t level = 1; fn > 0; ++level) {
         if (!bottom_up && (double)frontier_edges > (double)unexplored / alpha) bottom_up = true;
         else if (bottom_up && (double)fn < (double)n / beta) bottom_up = false;
-        PC_CUDA(cudaMemsetAsync(cnt, 0, 4, s));
+        PC_CUDA(cudaMemsetAsync(cnt, 0, 8, s));
         PC_CUDA(cudaMemsetAsync(edges, 0, 8, s));
         if (bottom_up) {
             k_bfs_bottom_up<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, n, dist, level, nq, cnt, edges);
         } else {
-            k_bfs_top_down<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, fq, fn, dist, level, nq, cnt, edges);
+            k_bfs_top_down<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, fq, fn, dist, level, nq, cnt, edges,
+                                                             hq, cnt + 1);
+            PC_LAUNCHED();
+            k_bfs_top_down_heavy<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, hq, cnt + 1, dist, level, nq, cnt,
+                                                                   edges);
         }
         PC_LAUNCHED();
         unsigned long long h_edges = 0;
@@ -477,7 +722,10 @@ template <class T>
 static pc_status pagerank_run(pc_pgraph* pg, T damping, int32_t iters, const T* init, T* out_host) {
     const uint64_t n = pg->g->n;
     cudaStream_t s = pg->g->stream;
-    PC_TRY(scratch_reserve(pg, n * sizeof(T) * 6 + 256));
+    const uint64_t hcap = heavy_cap(n, pg->g->m);
+    PC_TRY(scratch_reserve(pg, n * sizeof(T) * 6 + hcap * 4 + 512));
+    int32_t* hq = pg->scratch.take<int32_t>(hcap);
+    uint32_t* d_hn = pg->scratch.take<uint32_t>(1);
     T* degs = pg->scratch.take<T>(n);
     T* c0 = pg->scratch.take<T>(n);
     T* c1 = pg->scratch.take<T>(n);
@@ -493,10 +741,12 @@ static pc_status pagerank_run(pc_pgraph* pg, T damping, int32_t iters, const T* 
     }
     k_pr_init<T><<<nb, kThreads, 0, s>>>(pg->off, n, damping, ini, degs, c0);
     PC_LAUNCHED();
+    uint32_t hn = 0;
+    PC_TRY(list_heavy_rows(pg, hq, d_hn, &hn));
     // (1 - damping) / n (src/Graph.cpp:1558), in fp64 like the row sums
     const double base = (1.0 - (double)damping) / (double)n;
     for (int32_t it = 0; it < iters; ++it) {
-        k_pr_iter<T><<<grid_for(pg, 16), kThreads, 0, s>>>(pg->off, pg->adj, n, base, degs, c0, x, c1);
+        k_pr_iter<T><<<grid_for(pg, 16), kThreads, 0, s>>>(pg->off, pg->adj, n, base, degs, c0, x, c1, hq, hn);
         PC_LAUNCHED();
         std::swap(c0, c1);
     }
@@ -523,6 +773,11 @@ static pc_status mis_run(pc_pgraph* pg, bool hashed, uint64_t seed, int32_t* res
         k_mis_prio<<<nb, kThreads, 0, s>>>(n, int2api, pc_graph_key(seed, PC_GEN_PRIORITY), hashed ? 1 : 0, prio);
         PC_LAUNCHED();
     }
+    const uint32_t* dp = nullptr;
+    if (!prio) {
+        PC_TRY(ensure_dplus(pg));
+        dp = pg->dplus.as<uint32_t>();
+    }
     PC_CUDA(cudaMemsetAsync(state, 0, n * 4, s));
     // all vertices start undecided
     k_iota<<<nb, kThreads, 0, s>>>(q0, n);
@@ -532,7 +787,7 @@ static pc_status mis_run(pc_pgraph* pg, bool hashed, uint64_t seed, int32_t* res
     int32_t* nq = q1;
     for (uint64_t round = 0; un > 0; ++round) {
         PC_CUDA(cudaMemsetAsync(cnt, 0, 4, s));
-        k_mis_round<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, prio, fq, un, state, nq, cnt);
+        k_mis_round<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, prio, dp, fq, un, state, nq, cnt);
         PC_LAUNCHED();
         PC_TRY(read_u32(pg, cnt, &un));
         std::swap(fq, nq);
@@ -569,13 +824,16 @@ pc_status pc_sssp(pc_pgraph* pg, int32_t src, int32_t* dist_host) {
     PC_TRY(use_device(pg->g));
     const int32_t isrc = to_internal_id(pg, src);
     cudaStream_t s = pg->g->stream;
-    PC_TRY(scratch_reserve(pg, n * 4 * 5 + 256));
+    const uint64_t hcap = heavy_cap(n, pg->g->m);
+    PC_TRY(scratch_reserve(pg, n * 4 * 5 + hcap * 4 + 256));
     int32_t* dist = pg->scratch.take<int32_t>(n);
     int32_t* flag = pg->scratch.take<int32_t>(n);
     int32_t* q0 = pg->scratch.take<int32_t>(n);
     int32_t* q1 = pg->scratch.take<int32_t>(n);
     int32_t* out = pg->scratch.take<int32_t>(n);
-    uint32_t* cnt = pg->scratch.take<uint32_t>(4);
+    int32_t* hq = pg->scratch.take<int32_t>(hcap);
+    uint32_t* cnt = pg->scratch.take<uint32_t>(4);  // [0] next frontier, [1] heavy list
+    if (!cnt) return fail(PC_ERR_OOM, "SSSP scratch plan exceeds its reservation");
     const unsigned nb = (unsigned)ceil_div(n, kThreads);
     k_fill_i32<<<nb, kThreads, 0, s>>>(dist, n, INT_MAX / 2);  // src/test.cpp:202-203
     PC_LAUNCHED();
@@ -587,8 +845,11 @@ pc_status pc_sssp(pc_pgraph* pg, int32_t src, int32_t* dist_host) {
     int32_t* fq = q0;
     int32_t* nq = q1;
     for (uint64_t round = 0; fn > 0; ++round) {
-        PC_CUDA(cudaMemsetAsync(cnt, 0, 4, s));
-        k_sssp_relax<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, pg->w, fq, fn, dist, flag, nq, cnt);
+        PC_CUDA(cudaMemsetAsync(cnt, 0, 8, s));
+        k_sssp_relax<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, pg->w, fq, fn, dist, flag, nq, cnt, hq,
+                                                       cnt + 1);
+        PC_LAUNCHED();
+        k_sssp_relax_heavy<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, pg->w, hq, cnt + 1, dist, flag, nq, cnt);
         PC_LAUNCHED();
         PC_TRY(read_u32(pg, cnt, &fn));
         if (fn) {
@@ -670,7 +931,8 @@ pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
         if (largest) *largest = 0;
         return PC_OK;
     }
-    PC_TRY(scratch_reserve(pg, n * 4 * 7 + sizeof(KState) * 3 + sizeof(GridBarrier) + 8));
+    const uint64_t hcap = heavy_cap(n, pg->g->m);
+    PC_TRY(scratch_reserve(pg, n * 4 * 7 + hcap * 8 + sizeof(KState) * 3 + sizeof(GridBarrier) + 8));
     int32_t* deg = pg->scratch.take<int32_t>(n);
     int32_t* core = pg->scratch.take<int32_t>(n);
     int32_t* rem0 = pg->scratch.take<int32_t>(n);
@@ -678,6 +940,8 @@ pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
     int32_t* f0 = pg->scratch.take<int32_t>(n);
     int32_t* f1 = pg->scratch.take<int32_t>(n);
     int32_t* out = pg->scratch.take<int32_t>(n);
+    int32_t* hq0 = pg->scratch.take<int32_t>(hcap);
+    int32_t* hq1 = pg->scratch.take<int32_t>(hcap);
     KState* S = pg->scratch.take<KState>(3);
     GridBarrier* gb = pg->scratch.take<GridBarrier>(1);
     uint64_t* d_steps = pg->scratch.take<uint64_t>(1);
@@ -699,16 +963,17 @@ pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
     PC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_kcore_persistent, kThreads, 0));
     if (per_sm < 1) return fail(PC_ERR_CUDA, "k-core kernel cannot be resident");
     const unsigned grid = (unsigned)(sm_count(pg->g->device) * std::min(per_sm, 4));
-    // every step either peels (lowering degrees) or advances the level, so n
-    // levels plus n peel rounds bound the steps
-    uint64_t max_steps = 2 * n + 8;
+    // a step scans a level, peels a frontier or peels set-aside heavy rows;
+    // each vertex enters a frontier and a heavy list at most once, so n
+    // levels plus 2n peel rounds bound the steps
+    uint64_t max_steps = 3 * n + 8;
     uint64_t limit_ns = kBarrierLimitNs;
     const uint64_t* off = pg->off;
     const int32_t* adj = pg->adj;
     uint64_t nn = n;
-    void* args[] = {(void*)&off, (void*)&adj, (void*)&nn, (void*)&deg, (void*)&core, (void*)&rem0, (void*)&rem1,
-                    (void*)&f0, (void*)&f1, (void*)&S, (void*)&gb, (void*)&max_steps, (void*)&limit_ns,
-                    (void*)&d_steps};
+    void* args[] = {(void*)&off,  (void*)&adj, (void*)&nn, (void*)&deg, (void*)&core, (void*)&rem0,
+                    (void*)&rem1, (void*)&f0,  (void*)&f1, (void*)&hq0, (void*)&hq1,  (void*)&S,
+                    (void*)&gb,   (void*)&max_steps, (void*)&limit_ns, (void*)&d_steps};
     PC_CUDA(cudaLaunchCooperativeKernel((const void*)k_kcore_persistent, dim3(grid), dim3(kThreads), args, 0, s));
     PC_LAUNCHED();
     GridBarrier hb{};
@@ -753,14 +1018,20 @@ pc_status pc_cdlp(pc_pgraph* pg, int32_t iterations, int32_t* labels) {
     const uint64_t n = pg->g->n;
     if (n == 0 || iterations == 0) return PC_OK;
     cudaStream_t s = pg->g->stream;
-    PC_TRY(scratch_reserve(pg, n * 4 * 3 + 256));
+    const uint64_t hcap = heavy_cap(n, pg->g->m);
+    PC_TRY(scratch_reserve(pg, n * 4 * 3 + hcap * 4 + 512));
     int32_t* a = pg->scratch.take<int32_t>(n);
     int32_t* b = pg->scratch.take<int32_t>(n);
     int32_t* c = pg->scratch.take<int32_t>(n);
+    int32_t* hq = pg->scratch.take<int32_t>(hcap);
+    uint32_t* d_hn = pg->scratch.take<uint32_t>(1);
+    if (!d_hn) return fail(PC_ERR_OOM, "CDLP scratch plan exceeds its reservation");
     PC_CUDA(cudaMemcpyAsync(c, labels, n * 4, cudaMemcpyHostToDevice, s));
     PC_TRY(gather_to_internal_i32(pg, c, a));
+    uint32_t hn = 0;
+    PC_TRY(list_heavy_rows(pg, hq, d_hn, &hn));
     for (int32_t it = 0; it < iterations; ++it) {
-        k_cdlp_iter<<<grid_for(pg, 16), kThreads, 0, s>>>(pg->off, pg->adj, n, a, b);
+        k_cdlp_iter<<<grid_for(pg, 16), kThreads, 0, s>>>(pg->off, pg->adj, n, a, b, hq, hn);
         PC_LAUNCHED();
         std::swap(a, b);
     }

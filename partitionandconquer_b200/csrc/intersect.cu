@@ -38,31 +38,40 @@ __device__ __forceinline__ uint32_t edge_count(const uint64_t* __restrict__ off,
     return ecnt[rv + lb(adj + rv, dplus[v], (int32_t)u)];
 }
 
-// Jaccard per entry (fp32 output of the fp64 formula) and LCC per row.
-__global__ void k_finalize(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
-                           const uint32_t* __restrict__ dplus, const uint32_t* __restrict__ ecnt, uint64_t n,
-                           float* __restrict__ jac, double* __restrict__ lcc) {
+// Largest row r in [lo, hi] with off[r] <= j (off[lo] <= j < off[hi + 1]):
+// the row that holds CSR entry j, empty rows skipped.
+__device__ __forceinline__ uint64_t row_of(const uint64_t* __restrict__ off, uint64_t lo, uint64_t hi, uint64_t j) {
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= j) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Jaccard per CSR entry (fp32 output of the fp64 formula).  The work is split
+// by entries, not rows: each warp takes kJacChunk consecutive entries, finds
+// the rows at both ends of its chunk, and each lane finds the row of its own
+// entries inside that span, so a hub row is spread over many warps instead
+// of serialising one.
+constexpr uint64_t kJacChunk = 256;
+__global__ void k_jaccard_entries(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                                  const uint32_t* __restrict__ dplus, const uint32_t* __restrict__ ecnt, uint64_t n,
+                                  uint64_t m, float* __restrict__ jac) {
     const int lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t u = warp; u < n; u += nwarps) {
-        const uint64_t b = off[u], e = off[u + 1];
-        const uint64_t du = e - b;
-        unsigned long long sum = 0;
-        for (uint64_t j = b + lane; j < e; j += 32) {
+    for (uint64_t c0 = warp * kJacChunk; c0 < m; c0 += nwarps * kJacChunk) {
+        const uint64_t c1 = min(c0 + kJacChunk, m);
+        uint64_t r = 0;
+        if (lane < 2) r = row_of(off, 0, n - 1, lane == 0 ? c0 : c1 - 1);
+        const uint64_t r0 = __shfl_sync(0xffffffffu, r, 0), r1 = __shfl_sync(0xffffffffu, r, 1);
+        for (uint64_t j = c0 + lane; j < c1; j += 32) {
+            const uint64_t u = row_of(off, r0, r1, j);
             const int32_t v = adj[j];
             const uint32_t c = edge_count(off, adj, dplus, ecnt, u, v, j);
-            sum += c;
-            if (jac) {
-                const uint64_t dv = off[v + 1] - off[v];
-                // src/Graph.cpp:808-809: c / (deg_u + deg_v - c), in double
-                jac[j] = (float)((double)c / ((double)(du + dv) - (double)c));
-            }
-        }
-        for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-        if (lcc && lane == 0) {
-            // src/Graph.cpp:833-838: d = 0 -> 0; else sum / (d (d - 1)) (d = 1 gives 0/0)
-            lcc[u] = du < 1 ? 0.0 : (double)sum / (double)(du * (du - 1));
+            const uint64_t du = off[u + 1] - off[u], dv = off[v + 1] - off[v];
+            // src/Graph.cpp:808-809: c / (deg_u + deg_v - c), in double
+            jac[j] = (float)((double)c / ((double)(du + dv) - (double)c));
         }
     }
 }
@@ -205,8 +214,8 @@ pc_status pc_jaccard_edges(pc_pgraph* pg, float* out) {
     PC_TRY(tc_edge_triangles(pg, PC_VARIANT_AUTO, ecnt.as<uint32_t>(), &T));
     PC_TRY(scratch_reserve(pg, m * 4 + 1024));
     float* jac = pg->scratch.take<float>(m);
-    k_finalize<<<sm_count(pg->g->device) * 16, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(),
-                                                             ecnt.as<uint32_t>(), n, jac, nullptr);
+    k_jaccard_entries<<<sm_count(pg->g->device) * 8, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(),
+                                                                   ecnt.as<uint32_t>(), n, m, jac);
     PC_LAUNCHED();
     // entries are in the graph's own CSR order (internal ids are the graph's ids)
     PC_CUDA(cudaMemcpyAsync(out, jac, m * 4, cudaMemcpyDeviceToHost, s));
