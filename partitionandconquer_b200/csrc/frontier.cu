@@ -54,6 +54,10 @@ constexpr uint32_t kHeavyDeg = 1024;
 constexpr uint32_t kHeavyChunk = 256;
 constexpr uint32_t kHeavyBatch = 2048;  // list entries per shared-memory prefix
 static_assert(kHeavyBatch % kThreads == 0, "prefix items per thread");
+// Pull kernels (PageRank, CDLP): rows of more than kPullHeavyDeg entries get a
+// CTA; the others kPullLanes lanes, so a warp keeps 4 rows in flight.
+constexpr uint32_t kPullHeavyDeg = 256;
+constexpr int kPullLanes = 8;
 
 // Calls body(u, j, valid) for the entries j of every row of hq[0..hn); the 32
 // lanes of a warp call it together (valid is false past a row's end), so the
@@ -99,13 +103,13 @@ __device__ __forceinline__ void heavy_rows(const uint64_t* __restrict__ off, con
     }
 }
 
-// Rows of more than kHeavyDeg entries (pull kernels give each a whole CTA).
-__global__ void k_heavy_list(const uint64_t* __restrict__ off, uint64_t n, int32_t* __restrict__ hq,
+// Rows of more than thr entries (the pull kernels give each a whole CTA).
+__global__ void k_heavy_list(const uint64_t* __restrict__ off, uint64_t n, uint32_t thr, int32_t* __restrict__ hq,
                              uint32_t* __restrict__ hn) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t nr = (n + 31) & ~31ull;
     for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < nr; u += stride) {
-        const bool heavy = u < n && off[u + 1] - off[u] > kHeavyDeg;
+        const bool heavy = u < n && off[u + 1] - off[u] > thr;
         warp_append(heavy, (int32_t)u, hq, hn);
     }
 }
@@ -299,8 +303,9 @@ __device__ __forceinline__ void pr_epilogue(uint64_t v, double base, double sum,
 // run in fp64 for both instances, so the fp32 vectors carry only their own
 // storage rounding (within 1e-6 relative of the FP64 recurrence at 20
 // iterations; fp32 row sums over hub in-lists drift past that).  Rows listed
-// in hq (more than kHeavyDeg entries) get a whole CTA each; the others a
-// warp.  Both reductions run in a fixed order, so results are reproducible.
+// in hq (more than kPullHeavyDeg entries) get a whole CTA each; the others
+// kPullLanes lanes.  Both reductions run in a fixed order, so results are
+// reproducible.
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_pr_iter(const uint64_t* __restrict__ off,
                                                       const int32_t* __restrict__ adj, uint64_t n, double base,
@@ -324,15 +329,23 @@ __global__ void __launch_bounds__(kThreads) k_pr_iter(const uint64_t* __restrict
         }
         __syncthreads();
     }
+    // the other rows: kPullLanes lanes each, 32 / kPullLanes rows per warp at once
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t v = warp; v < n; v += nwarps) {
-        const uint64_t b = off[v], e = off[v + 1];
-        if (e - b > kHeavyDeg) continue;
+    constexpr int kRows = 32 / kPullLanes;
+    const int g = lane / kPullLanes, gl = lane % kPullLanes;
+    for (uint64_t v0 = warp * kRows; v0 < n; v0 += nwarps * kRows) {
+        const uint64_t v = v0 + g;
+        uint64_t b = 0, e = 0;
+        if (v < n) {
+            b = off[v];
+            e = off[v + 1];
+            if (e - b > kPullHeavyDeg) e = b;  // a CTA row
+        }
         double s = 0.0;
-        for (uint64_t j = b + lane; j < e; j += 32) s += (double)__ldg(contrib + adj[j]);
-        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) pr_epilogue(v, base, s, degs, x_out, contrib_out);
+        for (uint64_t j = b + gl; j < e; j += kPullLanes) s += (double)__ldg(contrib + adj[j]);
+        for (int o = kPullLanes / 2; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (v < n && gl == 0 && off[v + 1] - off[v] <= kPullHeavyDeg) pr_epilogue(v, base, s, degs, x_out, contrib_out);
     }
 }
 
@@ -593,7 +606,7 @@ __global__ void k_mis_finish(const int32_t* __restrict__ state, uint64_t n, int3
 
 // One iteration: out[v] = max label over N(v), 0 for an isolated vertex
 // (src/Graph.cpp:650: labels start at 0 for every vertex).  Rows listed in hq
-// get a whole CTA each; the others a warp.
+// get a whole CTA each; the others kPullLanes lanes.
 __global__ void __launch_bounds__(kThreads) k_cdlp_iter(const uint64_t* __restrict__ off,
                                                         const int32_t* __restrict__ adj, uint64_t n,
                                                         const int32_t* __restrict__ lab, int32_t* __restrict__ out,
@@ -617,13 +630,20 @@ __global__ void __launch_bounds__(kThreads) k_cdlp_iter(const uint64_t* __restri
     }
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t v = warp; v < n; v += nwarps) {
-        const uint64_t b = off[v], e = off[v + 1];
-        if (e - b > kHeavyDeg) continue;
+    constexpr int kRows = 32 / kPullLanes;
+    const int g = lane / kPullLanes, gl = lane % kPullLanes;
+    for (uint64_t v0 = warp * kRows; v0 < n; v0 += nwarps * kRows) {
+        const uint64_t v = v0 + g;
+        uint64_t b = 0, e = 0;
+        if (v < n) {
+            b = off[v];
+            e = off[v + 1];
+            if (e - b > kPullHeavyDeg) e = b;  // a CTA row
+        }
         int32_t mx = 0;
-        for (uint64_t j = b + lane; j < e; j += 32) mx = max(mx, __ldg(lab + adj[j]));
-        for (int o = 16; o; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        if (lane == 0) out[v] = mx;
+        for (uint64_t j = b + gl; j < e; j += kPullLanes) mx = max(mx, __ldg(lab + adj[j]));
+        for (int o = kPullLanes / 2; o; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (v < n && gl == 0 && off[v + 1] - off[v] <= kPullHeavyDeg) out[v] = mx;
     }
 }
 
@@ -635,14 +655,17 @@ static unsigned grid_for(const pc_pgraph* pg, int per_sm = 8) { return (unsigned
 
 // Entries a heavy list can need: rows of more than kHeavyDeg entries.
 static uint64_t heavy_cap(uint64_t n, uint64_t m) { return std::max<uint64_t>(1, std::min<uint64_t>(n, m / kHeavyDeg + 1)); }
+static uint64_t pull_heavy_cap(uint64_t n, uint64_t m) {
+    return std::max<uint64_t>(1, std::min<uint64_t>(n, m / kPullHeavyDeg + 1));
+}
 
-// Lists the rows of more than kHeavyDeg entries into hq (room for heavy_cap
-// entries) and reads their number back.
+// Lists the rows of more than kPullHeavyDeg entries into hq (room for
+// pull_heavy_cap entries) and reads their number back.
 static pc_status list_heavy_rows(pc_pgraph* pg, int32_t* hq, uint32_t* d_hn, uint32_t* hn) {
     if (!hq || !d_hn) return fail(PC_ERR_OOM, "scratch plan exceeds its reservation");
     cudaStream_t s = pg->g->stream;
     PC_CUDA(cudaMemsetAsync(d_hn, 0, 4, s));
-    k_heavy_list<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->g->n, hq, d_hn);
+    k_heavy_list<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->g->n, kPullHeavyDeg, hq, d_hn);
     PC_LAUNCHED();
     PC_CUDA(cudaMemcpyAsync(hn, d_hn, 4, cudaMemcpyDeviceToHost, s));
     PC_CUDA(cudaStreamSynchronize(s));
@@ -722,7 +745,7 @@ template <class T>
 static pc_status pagerank_run(pc_pgraph* pg, T damping, int32_t iters, const T* init, T* out_host) {
     const uint64_t n = pg->g->n;
     cudaStream_t s = pg->g->stream;
-    const uint64_t hcap = heavy_cap(n, pg->g->m);
+    const uint64_t hcap = pull_heavy_cap(n, pg->g->m);
     PC_TRY(scratch_reserve(pg, n * sizeof(T) * 6 + hcap * 4 + 512));
     int32_t* hq = pg->scratch.take<int32_t>(hcap);
     uint32_t* d_hn = pg->scratch.take<uint32_t>(1);
@@ -1018,7 +1041,7 @@ pc_status pc_cdlp(pc_pgraph* pg, int32_t iterations, int32_t* labels) {
     const uint64_t n = pg->g->n;
     if (n == 0 || iterations == 0) return PC_OK;
     cudaStream_t s = pg->g->stream;
-    const uint64_t hcap = heavy_cap(n, pg->g->m);
+    const uint64_t hcap = pull_heavy_cap(n, pg->g->m);
     PC_TRY(scratch_reserve(pg, n * 4 * 3 + hcap * 4 + 512));
     int32_t* a = pg->scratch.take<int32_t>(n);
     int32_t* b = pg->scratch.take<int32_t>(n);

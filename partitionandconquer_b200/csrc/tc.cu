@@ -596,7 +596,8 @@ static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long l
     if (is_bitmap(v)) {
         BitmapLaunch L;
         const size_t nsets = (size_t)(kCtaThreads / 32 / sh.K);
-        L.smem = sh.smem + (d_tri ? (size_t)kHubHist * 4 : 0) + (d_ecnt ? nsets * ((sh.words + 7) / 8) * 4 : 0);
+        L.smem = sh.smem + (d_tri ? (size_t)kHubHist * 4 : 0) +
+                 (d_ecnt ? nsets * (((sh.words + 7) / 8) + (size_t)kEcRankCap) * 4 : 0);
         const int cps = (d_tri || d_ecnt)
                             ? (int)std::max<size_t>(1, std::min<size_t>(4, (220 * 1024) / (L.smem + 1024)))
                             : sh.ctas_per_sm;

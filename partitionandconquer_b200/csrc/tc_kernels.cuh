@@ -33,6 +33,7 @@ constexpr int kCtaThreads = 512;    // threads per CTA of the bitmap kernels
 constexpr int kHashSlots = 512;     // slots per warp-private hash table
 constexpr int kHashCap = 256;       // max pivot set size for the hash kernel
 constexpr int kWarpCtaWarps = 8;    // warps per CTA of the warp kernels
+constexpr int kEcRankCap = 512;     // per-edge mode: pivot sets up to this size count by rank in shared memory
 constexpr int kHubHist = 8192;      // per-vertex counting: ids below this count in shared memory
 
 enum WarpMode { kModeHash = 0, kModeMerge = 1, kModeGallop = 2 };
@@ -173,8 +174,14 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
     // 256-id superblock (only those are ever read)
     const uint32_t nsb = (bm_words + 7) / 8;
     uint32_t* sb = smem + (size_t)nsets * bm_words + (size_t)set * nsb;
+    // kEC: per set, hits by rank in the pivot set (sets up to kEcRankCap),
+    // flushed to the row's slots once per item
+    uint32_t* ecs = smem + (size_t)nsets * (bm_words + nsb) + (size_t)set * kEcRankCap;
     const uint32_t zero_words = (uint32_t)nsets * bm_words + (kVC ? (uint32_t)kHubHist : 0u);
     for (uint32_t i = tid; i < zero_words; i += blockDim.x) smem[i] = 0;
+    if (kEC)
+        for (uint32_t i = tid; i < (uint32_t)nsets * kEcRankCap; i += blockDim.x)
+            smem[(size_t)nsets * (bm_words + nsb) + i] = 0;
     __syncthreads();
     auto set_sync = [&]() {
         if constexpr (K == 1) __syncwarp();
@@ -221,7 +228,8 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
                 if (j >= nb) limj = 0;
                 if (kEC) {
                     if (limj) cnt += scan_prefix_pipelined<G, false, true>(adj + rcj, limj, b, gl, gmask, bm, nullptr,
-                                                                           nullptr, ecnt + rcj, ecnt + rb, sb);
+                                                                           nullptr, ecnt + rcj,
+                                                                           dp <= kEcRankCap ? ecs : ecnt + rb, sb);
                 } else if (kVC) {
                     const int32_t cj = __shfl_sync(0xffffffffu, c, src);
                     if (limj) {
@@ -240,7 +248,16 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
             if (lane == 0 && hb) atomicAdd(&tri[b], hb);
         }
         set_sync();
-        for (uint32_t k = tis; k < dp; k += set_threads) bm[adj[rb + k] >> 5] = 0;
+        for (uint32_t k = tis; k < dp; k += set_threads) {
+            bm[adj[rb + k] >> 5] = 0;
+            if (kEC && dp <= kEcRankCap) {
+                const uint32_t h = ecs[k];
+                if (h) {
+                    atomicAdd(&ecnt[rb + k], h);
+                    ecs[k] = 0;
+                }
+            }
+        }
         set_sync();
         // profiling runs: the set's warp-cycles on this item, charged to its unit
         if (unit_cost && tis == 0) atomicAdd(&unit_cost[unit_of[b]], (unsigned long long)(clock64() - t0) * K);
@@ -396,16 +413,22 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
                                                                 uint32_t* __restrict__ ecnt = nullptr) {
     __shared__ int32_t table[MODE == kModeHash ? kWarpCtaWarps : 1][MODE == kModeHash ? kHashSlots : 1];
     __shared__ int32_t tpos[MODE == kModeHash && kEC ? kWarpCtaWarps : 1][MODE == kModeHash && kEC ? kHashSlots : 1];
+    // kEC: per warp, the hits of the pivot set's entries by rank, flushed to
+    // their slots once per item instead of one global atomic per triangle
+    __shared__ uint32_t rcnt[MODE == kModeHash && kEC ? kWarpCtaWarps : 1][MODE == kModeHash && kEC ? kHashCap : 1];
     __shared__ uint32_t hist[kVC ? kHubHist : 1];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int32_t* T = table[MODE == kModeHash ? w : 0];
     int32_t* TP = tpos[MODE == kModeHash && kEC ? w : 0];  // kEC: position of each key in N+(b)
+    uint32_t* RC = rcnt[MODE == kModeHash && kEC ? w : 0];
     if (kVC) {
         for (int i = threadIdx.x; i < kHubHist; i += blockDim.x) hist[i] = 0;
         __syncthreads();
     }
     if (MODE == kModeHash) {
         for (int s = lane; s < kHashSlots; s += 32) T[s] = -1;
+        if (kEC)
+            for (int s = lane; s < kHashCap; s += 32) RC[s] = 0;
         __syncwarp();
     }
     const uint32_t nitems = *nitems_p;
@@ -449,7 +472,7 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
                             if (kVC) count_vertex(a, tri, hist);
                             if (kEC) {
                                 atomicAdd(&ecnt[rc + i], 1u);
-                                atomicAdd(&ecnt[rb + TP[s]], 1u);
+                                atomicAdd(&RC[TP[s]], 1u);
                             }
                             break;
                         }
@@ -462,6 +485,15 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
             }
             __syncwarp();
             for (int s = lane; s < kHashSlots; s += 32) T[s] = -1;
+            if (kEC) {
+                for (uint32_t k = lane; k < dp; k += 32) {
+                    const uint32_t h = RC[k];
+                    if (h) {
+                        atomicAdd(&ecnt[rb + k], h);
+                        RC[k] = 0;
+                    }
+                }
+            }
             __syncwarp();
         } else if (MODE == kModeGallop) {
             for (uint64_t e = in0 + lane; e < in1; e += 32) {
