@@ -58,6 +58,7 @@ static_assert(kHeavyBatch % kThreads == 0, "prefix items per thread");
 // CTA; the others kPullLanes lanes, so a warp keeps 4 rows in flight.
 constexpr uint32_t kPullHeavyDeg = 256;
 constexpr int kPullLanes = 8;
+constexpr int kMisLanes = 8;  // MIS under id priorities: lanes per vertex
 
 // Calls body(u, j, valid) for the entries j of every row of hq[0..hn); the 32
 // lanes of a warp call it together (valid is false past a row's end), so the
@@ -558,13 +559,51 @@ __global__ void k_mis_round(const uint64_t* __restrict__ off, const int32_t* __r
     const int lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    if (dplus) {
+        // With id priorities only the neighbours below u matter: an IN
+        // neighbour v > u would need u OUT first, and only v < u block (rows
+        // are sorted, so those are the first dplus[u] entries).  Those lists
+        // are short, so kMisLanes lanes take a vertex, 32 / kMisLanes at once.
+        constexpr int kRows = 32 / kMisLanes;
+        const int g = lane / kMisLanes, gl = lane % kMisLanes;
+        const unsigned gm = ((1u << kMisLanes) - 1u) << (g * kMisLanes);
+        for (uint64_t i0 = warp * kRows; i0 < un; i0 += nwarps * kRows) {
+            const uint64_t i = i0 + g;
+            const bool have = i < un;
+            int32_t u = 0;
+            uint64_t b = 0, e = 0;
+            if (have) {
+                u = uq[i];
+                b = off[u];
+                e = b + dplus[u];
+            }
+            bool in_nbr = false, blocked = false;
+            for (uint64_t k = 0;; k += kMisLanes) {
+                const uint64_t j = b + k + gl;
+                bool a = false, c = false;
+                if (have && !in_nbr && j < e) {
+                    const int32_t v = adj[j];
+                    const int32_t sv = state[v];
+                    a = sv == 1;
+                    c = sv == 0;  // every v here is below u
+                }
+                in_nbr = in_nbr || (__ballot_sync(0xffffffffu, a) & gm);
+                blocked = blocked || (__ballot_sync(0xffffffffu, c) & gm);
+                const bool more = have && !in_nbr && b + k + kMisLanes < e;
+                if (!__any_sync(0xffffffffu, more)) break;
+            }
+            if (have && gl == 0) {
+                if (in_nbr) state[u] = 2;
+                else if (!blocked) state[u] = 1;
+            }
+            warp_append(have && gl == 0 && !in_nbr && blocked, u, nq, nn);
+        }
+        return;
+    }
     for (uint64_t i = warp; i < un; i += nwarps) {
         const int32_t u = uq[i];
         const uint64_t pu = prio ? prio[u] : (uint64_t)u;
-        // with id priorities only the neighbours below u matter: an IN
-        // neighbour v > u would need u OUT first, and only v < u block
-        // (rows are sorted, so those are the first dplus[u] entries)
-        const uint64_t b = off[u], e = dplus ? b + dplus[u] : off[u + 1];
+        const uint64_t b = off[u], e = off[u + 1];
         bool in_nbr = false, blocked = false;
         for (uint64_t j0 = b; j0 < e; j0 += 32) {
             const uint64_t j = j0 + lane;
