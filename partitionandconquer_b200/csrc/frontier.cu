@@ -587,8 +587,12 @@ __global__ void k_mis_round(const uint64_t* __restrict__ off, const int32_t* __r
                     a = sv == 1;
                     c = sv == 0;  // every v here is below u
                 }
-                in_nbr = in_nbr || (__ballot_sync(0xffffffffu, a) & gm);
-                blocked = blocked || (__ballot_sync(0xffffffffu, c) & gm);
+                // every lane votes (a short-circuit here would skip the
+                // vote on some lanes and leave the others waiting)
+                const unsigned va = __ballot_sync(0xffffffffu, a);
+                const unsigned vc = __ballot_sync(0xffffffffu, c);
+                in_nbr = in_nbr || (va & gm) != 0;
+                blocked = blocked || (vc & gm) != 0;
                 const bool more = have && !in_nbr && b + k + kMisLanes < e;
                 if (!__any_sync(0xffffffffu, more)) break;
             }
