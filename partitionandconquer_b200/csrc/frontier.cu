@@ -24,6 +24,7 @@ constexpr int32_t kInf = INT_MAX;
 constexpr uint64_t kBarrierLimitNs = 4000000000ull;
 // k-core: ids below this have their degree decrements gathered per CTA
 constexpr int kKcoreHubs = 4096;
+constexpr uint32_t kLocalQ = 1024;  // k-core: per-CTA queue of vertices pushed in a step
 static_assert(kKcoreHubs % kThreads == 0, "the flush loop needs a uniform trip count");
 
 // Appends `val` for every lane with pred set; all 32 lanes of the warp must
@@ -405,8 +406,14 @@ __global__ void __launch_bounds__(kThreads) k_kcore_persistent(
     // are gathered per CTA in shared memory and applied once per step
     __shared__ int32_t s_dec[kKcoreHubs];
     __shared__ int s_any;
+    __shared__ int32_t s_lq[2][kLocalQ];
+    __shared__ uint32_t s_lqn[2];
     for (int i = threadIdx.x; i < kKcoreHubs; i += blockDim.x) s_dec[i] = 0;
-    if (threadIdx.x == 0) s_any = 0;
+    if (threadIdx.x == 0) {
+        s_any = 0;
+        s_lqn[0] = 0;
+        s_lqn[1] = 0;
+    }
     __syncthreads();
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
     const int lane = threadIdx.x & 31;
@@ -439,6 +446,22 @@ __global__ void __launch_bounds__(kThreads) k_kcore_persistent(
             int32_t* nq = in.fpar ? f0 : f1;
             int32_t* hq_next = (step & 1) ? hq1 : hq0;
             const int32_t* hq_prev = (step & 1) ? hq0 : hq1;
+            // A vertex pushed at this level goes to this CTA's local queue
+            // (s_lq[wr]) while it has room, else to the next step's frontier;
+            // the CTA peels its local queue itself, so a level's cascade
+            // takes one step instead of one step per round.
+            int wr = 0;
+            auto push_v = [&](bool pred, int32_t v) {
+                const unsigned m = __ballot_sync(0xffffffffu, pred);
+                if (!m) return;
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(&s_lqn[wr], (uint32_t)__popc(m));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                const uint32_t idx = base + __popc(m & ((1u << lane) - 1u));
+                const bool local = pred && idx < kLocalQ;
+                if (local) s_lq[wr][idx] = v;
+                warp_append(pred && !local, v, nq, &out->fn);
+            };
             // one CSR entry (u, v) of a peeled vertex u; all lanes call it
             auto peel_entry = [&](uint64_t j, bool ok) {
                 bool push = false;
@@ -458,37 +481,58 @@ __global__ void __launch_bounds__(kThreads) k_kcore_persistent(
                         }
                     }
                 }
-                warp_append(push, v, nq, &out->fn);
+                push_v(push, v);
             };
-            for (uint64_t i = warp; i < in.fn; i += nwarps) {
-                const int32_t u = __ldcg(fq + i);
+            // the row of a peeled vertex u, by one warp (set aside if heavy)
+            auto peel_row = [&](int32_t u) {
                 const uint64_t b = off[u], e = off[u + 1];
                 if (e - b > kHeavyDeg) {
                     if (lane == 0) hq_next[atomicAdd(&out->hn, 1u)] = u;
-                    continue;
+                    return;
                 }
                 for (uint64_t j0 = b; j0 < e; j0 += 32) peel_entry(j0 + lane, j0 + lane < e);
-            }
+            };
+            for (uint64_t i = warp; i < in.fn; i += nwarps) peel_row(__ldcg(fq + i));
             heavy_rows(off, hq_prev, in.hn, [&](int32_t, uint64_t j, bool ok) { peel_entry(j, ok); });
-            // flush the gathered hub decrements: the one flush that takes a
-            // degree from >= k to < k pushes the vertex
-            __syncthreads();
-            if (s_any) {
-                for (int i = threadIdx.x; i < kKcoreHubs; i += blockDim.x) {
-                    const int32_t c = s_dec[i];
-                    bool push = false;
-                    if (c) {
-                        s_dec[i] = 0;
-                        const int32_t old = atomicSub(&deg[i], c);
-                        if (old >= k && old - c < k) {
-                            push = true;
-                            core[i] = k - 1;
-                        }
-                    }
-                    warp_append(push, i, nq, &out->fn);
-                }
+            // drain the local queues; when one runs dry, flush the gathered
+            // hub decrements (the one flush that takes a degree from >= k to
+            // < k pushes the vertex) and go on until nothing is left
+            int rd = 0;
+            for (;;) {
                 __syncthreads();
-                if (threadIdx.x == 0) s_any = 0;
+                uint32_t cnt = min(s_lqn[rd], (uint32_t)kLocalQ);
+                if (cnt == 0) {
+                    if (s_any) {
+                        wr = rd;
+                        for (int i = threadIdx.x; i < kKcoreHubs; i += blockDim.x) {
+                            const int32_t c = s_dec[i];
+                            bool push = false;
+                            if (c) {
+                                s_dec[i] = 0;
+                                const int32_t old = atomicSub(&deg[i], c);
+                                if (old >= k && old - c < k) {
+                                    push = true;
+                                    core[i] = k - 1;
+                                }
+                            }
+                            push_v(push, i);
+                        }
+                        __syncthreads();
+                        if (threadIdx.x == 0) s_any = 0;
+                        __syncthreads();
+                        cnt = min(s_lqn[rd], (uint32_t)kLocalQ);
+                    }
+                    if (cnt == 0) break;
+                }
+                wr = rd ^ 1;
+                for (uint32_t i = threadIdx.x >> 5; i < cnt; i += blockDim.x >> 5) peel_row(s_lq[rd][i]);
+                __syncthreads();
+                if (threadIdx.x == 0) s_lqn[rd] = 0;
+                rd ^= 1;
+            }
+            if (threadIdx.x == 0) {
+                s_lqn[0] = 0;
+                s_lqn[1] = 0;
             }
         } else {
             // scan of level k over the remaining list
@@ -504,7 +548,9 @@ __global__ void __launch_bounds__(kThreads) k_kcore_persistent(
                     if (__ldcg(core + u) < 0) {
                         const int32_t d = __ldcg(deg + u);
                         if (d < k) {
-                            pl = true;
+                            // d counts the unpeeled neighbours: with none,
+                            // peeling u would decrement nobody
+                            pl = d > 0;
                             core[u] = k - 1;
                         } else {
                             keep = true;
@@ -541,9 +587,16 @@ __global__ void k_grid_sync_selftest(GridBarrier* gb, int rounds, int absent, ui
     }
 }
 
-__global__ void k_kcore_unpeeled(int32_t* __restrict__ core, uint64_t n) {
-    uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (u < n && core[u] < 0) core[u] = 0;
+// Vertices never peeled get core 0; *top receives the largest core number.
+__global__ void k_kcore_finish(int32_t* __restrict__ core, uint64_t n, int32_t* __restrict__ top) {
+    const uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    int32_t c = 0;
+    if (u < n) {
+        c = core[u];
+        if (c < 0) core[u] = c = 0;
+    }
+    for (int o = 16; o; o >>= 1) c = max(c, __shfl_xor_sync(0xffffffffu, c, o));
+    if ((threadIdx.x & 31) == 0 && c > 0) atomicMax(top, c);
 }
 
 // ---- MIS -------------------------------------------------------------------------
@@ -998,7 +1051,7 @@ pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
         return PC_OK;
     }
     const uint64_t hcap = heavy_cap(n, pg->g->m);
-    PC_TRY(scratch_reserve(pg, n * 4 * 7 + hcap * 8 + sizeof(KState) * 3 + sizeof(GridBarrier) + 8));
+    PC_TRY(scratch_reserve(pg, n * 4 * 7 + hcap * 8 + sizeof(KState) * 3 + sizeof(GridBarrier) + 16));
     int32_t* deg = pg->scratch.take<int32_t>(n);
     int32_t* core = pg->scratch.take<int32_t>(n);
     int32_t* rem0 = pg->scratch.take<int32_t>(n);
@@ -1011,7 +1064,8 @@ pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
     KState* S = pg->scratch.take<KState>(3);
     GridBarrier* gb = pg->scratch.take<GridBarrier>(1);
     uint64_t* d_steps = pg->scratch.take<uint64_t>(1);
-    if (!d_steps) return fail(PC_ERR_OOM, "k-core scratch plan exceeds its reservation");
+    int32_t* d_top = pg->scratch.take<int32_t>(1);
+    if (!d_top) return fail(PC_ERR_OOM, "k-core scratch plan exceeds its reservation");
     const unsigned nb = (unsigned)ceil_div(n, kThreads);
     k_kcore_init<<<nb, kThreads, 0, s>>>(pg->off, n, deg, core, rem0);
     PC_LAUNCHED();
@@ -1025,6 +1079,7 @@ pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
     init[1].ml = INT_MAX;
     PC_CUDA(cudaMemcpyAsync(S, init, sizeof(init), cudaMemcpyHostToDevice, s));
     PC_CUDA(cudaMemsetAsync(gb, 0, sizeof(GridBarrier), s));
+    PC_CUDA(cudaMemsetAsync(d_top, 0, 4, s));
     int per_sm = 0;
     PC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_kcore_persistent, kThreads, 0));
     if (per_sm < 1) return fail(PC_ERR_CUDA, "k-core kernel cannot be resident");
@@ -1042,21 +1097,19 @@ pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
                     (void*)&gb,   (void*)&max_steps, (void*)&limit_ns, (void*)&d_steps};
     PC_CUDA(cudaLaunchCooperativeKernel((const void*)k_kcore_persistent, dim3(grid), dim3(kThreads), args, 0, s));
     PC_LAUNCHED();
-    GridBarrier hb{};
-    PC_CUDA(cudaMemcpyAsync(&hb, gb, sizeof(hb), cudaMemcpyDeviceToHost, s));
-    PC_CUDA(cudaStreamSynchronize(s));
-    if (hb.err == 1) return fail(PC_ERR_TIMEOUT, "k-core: a grid barrier wait ran out of time");
-    if (hb.err) return fail(PC_ERR_TIMEOUT, "k-core peeling did not finish within its step bound");
-    k_kcore_unpeeled<<<nb, kThreads, 0, s>>>(core, n);
+    k_kcore_finish<<<nb, kThreads, 0, s>>>(core, n, d_top);
     PC_LAUNCHED();
     PC_TRY(gather_to_api_i32(pg, core, out));
     PC_CUDA(cudaMemcpyAsync(core_host, out, n * 4, cudaMemcpyDeviceToHost, s));
+    GridBarrier hb{};
+    int32_t top = 0;
+    PC_CUDA(cudaMemcpyAsync(&hb, gb, sizeof(hb), cudaMemcpyDeviceToHost, s));
+    PC_CUDA(cudaMemcpyAsync(&top, d_top, 4, cudaMemcpyDeviceToHost, s));
     PC_TRY(sync(pg));
-    if (largest) {
-        int32_t top = 0;
-        for (uint64_t u = 0; u < n; ++u) top = std::max(top, core_host[u]);
-        *largest = top;
-    }
+    // the kernel's own status decides whether core_host holds a result
+    if (hb.err == 1) return fail(PC_ERR_TIMEOUT, "k-core: a grid barrier wait ran out of time");
+    if (hb.err) return fail(PC_ERR_TIMEOUT, "k-core peeling did not finish within its step bound");
+    if (largest) *largest = top;
     return PC_OK;
 }
 
