@@ -24,7 +24,8 @@ constexpr int32_t kInf = INT_MAX;
 constexpr uint64_t kBarrierLimitNs = 4000000000ull;
 // k-core: ids below this have their degree decrements gathered per CTA
 constexpr int kKcoreHubs = 4096;
-constexpr uint32_t kLocalQ = 1024;  // k-core: per-CTA queue of vertices pushed in a step
+constexpr uint32_t kLocalQ = 1024;       // k-core: per-CTA queue of vertices pushed in a step
+constexpr uint32_t kLocalEdges = 16384;  // ... peeled by the CTA itself while their rows stay below this
 static_assert(kKcoreHubs % kThreads == 0, "the flush loop needs a uniform trip count");
 
 // Appends `val` for every lane with pred set; all 32 lanes of the warp must
@@ -407,12 +408,13 @@ __global__ void __launch_bounds__(kThreads) k_kcore_persistent(
     __shared__ int32_t s_dec[kKcoreHubs];
     __shared__ int s_any;
     __shared__ int32_t s_lq[2][kLocalQ];
-    __shared__ uint32_t s_lqn[2];
+    __shared__ uint32_t s_lqn[2];  // entries pushed (may exceed kLocalQ: the rest went to the frontier)
+    __shared__ uint32_t s_lqe[2];  // row entries of the queued vertices
     for (int i = threadIdx.x; i < kKcoreHubs; i += blockDim.x) s_dec[i] = 0;
     if (threadIdx.x == 0) {
         s_any = 0;
-        s_lqn[0] = 0;
-        s_lqn[1] = 0;
+        s_lqn[0] = s_lqn[1] = 0;
+        s_lqe[0] = s_lqe[1] = 0;
     }
     __syncthreads();
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
@@ -459,7 +461,13 @@ __global__ void __launch_bounds__(kThreads) k_kcore_persistent(
                 base = __shfl_sync(0xffffffffu, base, 0);
                 const uint32_t idx = base + __popc(m & ((1u << lane) - 1u));
                 const bool local = pred && idx < kLocalQ;
-                if (local) s_lq[wr][idx] = v;
+                uint32_t len = 0;
+                if (local) {
+                    s_lq[wr][idx] = v;
+                    len = (uint32_t)min(off[v + 1] - off[v], (uint64_t)kHeavyDeg + 1);
+                }
+                for (int o = 16; o; o >>= 1) len += __shfl_xor_sync(0xffffffffu, len, o);
+                if (lane == 0 && len) atomicAdd(&s_lqe[wr], len);
                 warp_append(pred && !local, v, nq, &out->fn);
             };
             // one CSR entry (u, v) of a peeled vertex u; all lanes call it
@@ -524,15 +532,30 @@ __global__ void __launch_bounds__(kThreads) k_kcore_persistent(
                     }
                     if (cnt == 0) break;
                 }
+                if (s_lqe[rd] > kLocalEdges) {
+                    // too much for one CTA: the next step shares it among all
+                    const uint32_t cpad = (cnt + 31) & ~31u;
+                    for (uint32_t i = threadIdx.x; i < cpad; i += blockDim.x)
+                        warp_append(i < cnt, i < cnt ? s_lq[rd][i] : 0, nq, &out->fn);
+                    __syncthreads();
+                    if (threadIdx.x == 0) {
+                        s_lqn[rd] = 0;
+                        s_lqe[rd] = 0;
+                    }
+                    continue;
+                }
                 wr = rd ^ 1;
                 for (uint32_t i = threadIdx.x >> 5; i < cnt; i += blockDim.x >> 5) peel_row(s_lq[rd][i]);
                 __syncthreads();
-                if (threadIdx.x == 0) s_lqn[rd] = 0;
+                if (threadIdx.x == 0) {
+                    s_lqn[rd] = 0;
+                    s_lqe[rd] = 0;
+                }
                 rd ^= 1;
             }
             if (threadIdx.x == 0) {
-                s_lqn[0] = 0;
-                s_lqn[1] = 0;
+                s_lqn[0] = s_lqn[1] = 0;
+                s_lqe[0] = s_lqe[1] = 0;
             }
         } else {
             // scan of level k over the remaining list
