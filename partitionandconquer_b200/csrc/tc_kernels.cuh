@@ -141,6 +141,77 @@ __device__ __forceinline__ uint32_t scan_prefix_pipelined(const int32_t* __restr
     return hits;
 }
 
+// The same scan with 16-byte loads, for groups of G < 32 lanes: each lane
+// takes 4 consecutive ids per step, so a group of 8 reads a whole 128-byte
+// line per dependent round instead of 32 bytes.  The row is read from the
+// 16-byte boundary at or below its start (positions before 0 are masked);
+// a load may run up to 3 ids past lim, which the adjacency array's padding
+// (64 ids after the last row) keeps in bounds.
+template <int G, bool kVC = false, bool kEC = false>
+__device__ __forceinline__ uint32_t scan_prefix_vec4(const int32_t* __restrict__ row, uint32_t lim, int32_t b, int gl,
+                                                     unsigned gmask, const uint32_t* __restrict__ bm,
+                                                     unsigned long long* __restrict__ tri = nullptr,
+                                                     uint32_t* hist = nullptr, uint32_t* __restrict__ ec_c = nullptr,
+                                                     uint32_t* __restrict__ ec_b = nullptr,
+                                                     const uint32_t* __restrict__ sb = nullptr) {
+    constexpr uint32_t kSpan = 4 * G;  // ids per group step
+    const uint32_t mis = (uint32_t)(reinterpret_cast<uintptr_t>(row) >> 2) & 3u;
+    const int4* q = reinterpret_cast<const int4*>(row - mis);
+    const uint32_t total = lim + mis;  // ids from q[0] to the end of the bound
+    const int4 none = make_int4(0x7fffffff, 0x7fffffff, 0x7fffffff, 0x7fffffff);
+    uint32_t hits = 0;
+    int32_t kb = -1;  // kEC: index of b in the row, seen by one lane of the group
+    uint32_t c0 = 0;
+    int4 v = 4u * gl < total ? __ldg(q + gl) : none;
+    for (;;) {
+        const uint32_t c1 = c0 + kSpan;
+        const int4 vn = c1 + 4u * gl < total ? __ldg(q + c1 / 4 + gl) : none;
+        const int32_t e[4] = {v.x, v.y, v.z, v.w};
+        bool stop = false;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int64_t pos = (int64_t)(c0 + 4u * gl + t) - (int64_t)mis;  // index in row
+            if (pos < 0 || pos >= (int64_t)lim) continue;
+            const int32_t a = e[t];
+            if (a < b) {
+                const uint32_t bit = (bm[a >> 5] >> (a & 31)) & 1u;
+                hits += bit;
+                if (kVC && bit) count_vertex(a, tri, hist);
+                if (kEC && bit) {
+                    atomicAdd(&ec_c[pos], 1u);
+                    atomicAdd(&ec_b[rank_in_set(bm, sb, a)], 1u);
+                }
+            } else {
+                stop = true;
+                if (kEC && a == b) kb = (int32_t)pos;
+            }
+        }
+        bool any_stop;
+        if constexpr (G == 1) any_stop = stop;
+        else any_stop = __any_sync(gmask, stop);
+        if (any_stop || c1 >= total) break;
+        v = vn;
+        c0 = c1;
+    }
+    if (kEC) {
+        const uint32_t sum = G == 1 ? hits : __reduce_add_sync(gmask, hits);
+        if (kb >= 0 && sum) atomicAdd(&ec_c[kb], sum);
+    }
+    return hits;
+}
+
+// The prefix scan a group of G lanes runs: 16-byte loads below 32 lanes.
+template <int G, bool kVC = false, bool kEC = false>
+__device__ __forceinline__ uint32_t scan_group_prefix(const int32_t* __restrict__ row, uint32_t lim, int32_t b, int gl,
+                                                      unsigned gmask, const uint32_t* __restrict__ bm,
+                                                      unsigned long long* __restrict__ tri = nullptr,
+                                                      uint32_t* hist = nullptr, uint32_t* __restrict__ ec_c = nullptr,
+                                                      uint32_t* __restrict__ ec_b = nullptr,
+                                                      const uint32_t* __restrict__ sb = nullptr) {
+    if constexpr (G < 32) return scan_prefix_vec4<G, kVC, kEC>(row, lim, b, gl, gmask, bm, tri, hist, ec_c, ec_b, sb);
+    else return scan_prefix_pipelined<G, kVC, kEC>(row, lim, b, gl, gmask, bm, tri, hist, ec_c, ec_b, sb);
+}
+
 // Bitmap kernel: a CTA of kCtaThreads threads holds 16/K pivot bitmaps in
 // shared memory, one per group of K warps; each group takes its own work
 // items (pivot, a run of its in-neighbours), so a group synchronises only
@@ -227,19 +298,19 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
                 uint32_t limj = __shfl_sync(0xffffffffu, lim, src);
                 if (j >= nb) limj = 0;
                 if (kEC) {
-                    if (limj) cnt += scan_prefix_pipelined<G, false, true>(adj + rcj, limj, b, gl, gmask, bm, nullptr,
+                    if (limj) cnt += scan_group_prefix<G, false, true>(adj + rcj, limj, b, gl, gmask, bm, nullptr,
                                                                            nullptr, ecnt + rcj,
                                                                            dp <= kEcRankCap ? ecs : ecnt + rb, sb);
                 } else if (kVC) {
                     const int32_t cj = __shfl_sync(0xffffffffu, c, src);
                     if (limj) {
-                        const uint32_t h = scan_prefix_pipelined<G, true>(adj + rcj, limj, b, gl, gmask, bm, tri, hist);
+                        const uint32_t h = scan_group_prefix<G, true>(adj + rcj, limj, b, gl, gmask, bm, tri, hist);
                         cnt += h;
                         hb += h;
                         if (h) atomicAdd(&tri[cj], (unsigned long long)h);
                     }
                 } else if (limj) {
-                    cnt += scan_prefix_pipelined<G>(adj + rcj, limj, b, gl, gmask, bm);
+                    cnt += scan_group_prefix<G>(adj + rcj, limj, b, gl, gmask, bm);
                 }
             }
         }
