@@ -531,10 +531,24 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
                 const uint64_t rc = off[c];
                 const int32_t* row = adj + rc;
                 const uint32_t lim = dplus[c];
-                uint32_t h = 0, i = 0;
-                for (; i < lim; ++i) {
-                    const int32_t a = __ldg(row + i);
-                    if (a >= b) break;
+                // the lane's prefix scan, 4 ids per 16-byte load with the
+                // next load in flight (read from the 16-byte boundary at or
+                // below the row start; the padding after the last row keeps
+                // the up to 3 ids past lim in bounds)
+                uint32_t h = 0, i = lim;  // i: index of the first id >= b
+                const uint32_t mis = (uint32_t)(reinterpret_cast<uintptr_t>(row) >> 2) & 3u;
+                const int4* q = reinterpret_cast<const int4*>(row - mis);
+                const uint32_t total = lim + mis;
+                int4 v = total ? __ldg(q) : make_int4(0, 0, 0, 0);
+                bool stop = false;
+                // one id of the prefix at index pos (masked outside [0, lim))
+                auto probe = [&](int32_t a, int64_t pos) {
+                    if (stop || pos < 0 || pos >= (int64_t)lim) return;
+                    if (a >= b) {
+                        stop = true;
+                        i = (uint32_t)pos;
+                        return;
+                    }
                     uint32_t s = hash_slot(a);
                     int32_t key;
                     while ((key = T[s]) != -1) {
@@ -542,13 +556,23 @@ __global__ void __launch_bounds__(kWarpCtaWarps * 32) k_tc_warp(const uint64_t* 
                             ++h;
                             if (kVC) count_vertex(a, tri, hist);
                             if (kEC) {
-                                atomicAdd(&ecnt[rc + i], 1u);
+                                atomicAdd(&ecnt[rc + pos], 1u);
                                 atomicAdd(&RC[TP[s]], 1u);
                             }
                             break;
                         }
                         s = (s + 1) & (kHashSlots - 1);
                     }
+                };
+                for (uint32_t c0 = 0; c0 < total; c0 += 4) {
+                    const int4 vn = c0 + 4 < total ? __ldg(q + c0 / 4 + 1) : v;
+                    const int64_t p0 = (int64_t)c0 - (int64_t)mis;
+                    probe(v.x, p0);
+                    probe(v.y, p0 + 1);
+                    probe(v.z, p0 + 2);
+                    probe(v.w, p0 + 3);
+                    if (stop) break;
+                    v = vn;
                 }
                 cnt += h;
                 if (kVC && h) atomicAdd(&tri[c], (unsigned long long)h);
