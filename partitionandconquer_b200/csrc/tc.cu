@@ -211,8 +211,23 @@ __device__ __forceinline__ unsigned long long matrix_pairs(const int32_t* __rest
                                                            int32_t lo, uint32_t hwords,
                                                            const uint32_t* __restrict__ H, uint32_t* Sb, int lane) {
     unsigned long long cnt = 0;
+    // Pivots at positions j < 32 have fewer than 32 probes each: their pairs
+    // (j, i), i < j, are numbered f = j (j - 1) / 2 + i and taken 32 at a
+    // time, so every lane probes instead of j of them per pivot.
+    const uint32_t jm = k < 32u ? k : 32u;
+    if (j0 < jm) {
+        const uint32_t f1 = jm * (jm - 1) / 2;
+        for (uint32_t f = j0 * (j0 - 1) / 2 + lane; f < f1; f += 32) {
+            uint32_t j = (uint32_t)((1.0f + sqrtf(1.0f + 8.0f * (float)f)) * 0.5f);
+            while (j * (j - 1) / 2 > f) --j;
+            while ((j + 1) * j / 2 <= f) ++j;
+            const int32_t b = S[j], a = S[f - j * (j - 1) / 2];
+            cnt += (H[(uint64_t)(b - lo) * hwords + (a >> 5)] >> (a & 31)) & 1u;
+        }
+    }
+    const uint32_t jr = j0 > jm ? j0 : jm;  // the per-pivot loop starts here
     bool want = false;
-    for (uint32_t j = j0 + lane; j < k; j += 32) want |= (uint32_t)((S[j] + 31) >> 5) <= j;
+    for (uint32_t j = jr + lane; j < k; j += 32) want |= (uint32_t)((S[j] + 31) >> 5) <= j;
     const bool words = __any_sync(0xffffffffu, want);
     if (words) {
         for (uint32_t i = lane; i < k; i += 32) {
@@ -221,7 +236,7 @@ __device__ __forceinline__ unsigned long long matrix_pairs(const int32_t* __rest
         }
         __syncwarp();
     }
-    for (uint32_t j = j0; j < k; ++j) {
+    for (uint32_t j = jr; j < k; ++j) {
         const int32_t b = S[j];
         const uint32_t* h = H + (uint64_t)(b - lo) * hwords;
         const uint32_t nw = (uint32_t)(b + 31) >> 5;
