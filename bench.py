@@ -11,10 +11,11 @@ graph.  Rank 0 prints one JSON line.
               learned per-partition selector (PC_VARIANT_AUTO).
  * e2e     -- the same through the C ABI from pinned host buffers: CSR upload
               (validated), partition view, plan, counting, 8-byte result read.
- * roofline -- SURVEY's algorithmic bytes of triangle counting,
-              B = 4 W + 12 |E+| + 8 (n+1) with W = sum over oriented edges of
-              (d+(u) + d+(v)), over the summed duration of the counting
-              kernels, against the measured HBM copy bandwidth.
+ * roofline -- the algorithmic bytes of the merge formulation of triangle
+              counting, B = 4 W + 12 |E+| + 8 (n+1) with W = sum over oriented
+              edges of (d+(u) + d+(v)), over the summed duration of the
+              counting kernels, against the measured HBM copy bandwidth
+              (MEASURED_PEAKS.json; the 6650 GB/s fallback when it is absent).
  * cpu_baseline -- the reference's own loop (Graph::solve_triangle_counting_merge,
               src/Graph.cpp:358-365, calling Graph::cnt_common_neis_less_than_merge)
               over an every-k-th-row sample on all host cores, extrapolated.
