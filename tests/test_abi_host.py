@@ -142,3 +142,24 @@ def test_equal_vertex_partition(pc):
     assert v.dtype == np.int32 and v.min() == 0 and v.max() == 63
     assert np.all(np.bincount(v) == 1024)
     assert np.all(np.diff(v) >= 0)
+
+
+def test_result_buffers_are_validated_on_the_host(pc):
+    """Every result method takes an optional caller-owned `out`; a buffer of
+    the wrong size, dtype, layout or writability is refused before any
+    device work, and a good one is used as is."""
+    from partitionandconquer_b200 import _result
+    got = _result(None, 5, np.int32)
+    assert got.dtype == np.int32 and got.size == 5
+    buf = np.zeros(7, np.float32)
+    assert _result(buf, 7, np.float32) is buf
+    for bad in (np.zeros(6, np.float32),              # size
+                np.zeros(7, np.float64),              # dtype
+                np.zeros(14, np.float32)[::2],        # not contiguous
+                [0.0] * 7):                           # not an array
+        with pytest.raises(ValueError):
+            _result(bad, 7, np.float32)
+    ro = np.zeros(7, np.float32)
+    ro.flags.writeable = False
+    with pytest.raises(ValueError):
+        _result(ro, 7, np.float32)
