@@ -260,7 +260,7 @@ def run_reference_arm(args, dist):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_s * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded RMAT)",
-        "config": {"workload": f"tc_rmat{args.scale}_ef{args.edge_factor}", "partitions": args.partitions,
+        "config": {"workload": f"tc_rmat{args.scale}_ef{args.edge_factor}_p{args.partitions}", "partitions": args.partitions,
                    "path": "Graph::solve_triangle_counting_merge loop (the partitioned constructor needs P*n "
                            "offsets plus 2*P*n vectors: infeasible in memory at this size)"},
         "cpu_baseline": {"value": round(value, 6), "unit": "GTEPS", "cores": threads, "kind": kind,
