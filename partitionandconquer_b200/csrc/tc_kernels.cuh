@@ -74,9 +74,6 @@ __device__ __forceinline__ void group_barrier(int id, int nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-// Pipelined group-of-G prefix scan: the load of the next G ids is issued
-// before the current ones are tested, so two loads per lane are in flight.
-// Stops at the first id >= b and never reads past lim = dplus[c].
 // Per-vertex triangle counts (kVC): every triangle found adds 1 to its
 // lowest vertex a; ids below kHubHist go to a shared-memory histogram
 // (almost every hit is a hub), the rest to the global counts.
@@ -95,6 +92,10 @@ __device__ __forceinline__ uint32_t rank_in_set(const uint32_t* __restrict__ bm,
     return r + __popc(bm[w] & ((1u << (a & 31)) - 1u));
 }
 
+// Pipelined group-of-G prefix scan (the 32-lane groups use it): the load of
+// the next G ids is issued before the current ones are tested, so two loads
+// per lane are in flight.  Stops at the first id >= b and never reads past
+// lim = dplus[c].
 // Modes of the pivot-form kernels: count only; kVC per-vertex triangle
 // counts (LCC); kEC per-edge counts at the oriented slots (Jaccard): every
 // triangle a < b < c adds 1 to the slot of a in row c (its scan index), to
