@@ -260,17 +260,20 @@ pc_status pc_cdlp(pc_pgraph* pg, int32_t iterations, int32_t* labels);
  * path must not risk an allocation's synchronisation or latency): the
  * triangle count -- each triangle once, as PC_METHOD_MERGE -- of a symmetric
  * CSR the caller already holds in device memory (d_vlist: n+1 uint64
- * offsets; d_elist: m int32 ids, rows strictly ascending, no self-loops; the
- * CSR is not validated).  Nothing is allocated: the temporaries live in a
- * fixed array inside the library image (about 4 MiB per GPU, held until the
- * process exits), which caps n at 2^20 vertices; larger graphs return
- * PC_ERR_INVALID_INPUT.  The first call on a device looks up that array's
- * device address (cudaGetSymbolAddress) with the device current; make that
- * first call before any stream capture.  Runs on the current device, on
- * `stream` (NULL: the legacy default stream), and returns once *count is
- * written.  Every call shares the array, which keeps the previous call's
- * contents (the counters are cleared at the start of each call): calls that
- * overlap on the GPU race. */
+ * offsets; d_elist: m int32 ids, rows strictly ascending, no self-loops).
+ * Nothing is allocated: the temporaries live in a fixed array inside the
+ * library image (about 4 MiB per GPU, held until the process exits), which
+ * caps n at 2^20 vertices; larger graphs return PC_ERR_INVALID_INPUT.  The
+ * CSR is checked only as far as memory safety needs (offsets non-decreasing
+ * and ending at m, neighbour ids in [0, n)); a violation returns
+ * PC_ERR_INVALID_INPUT.  Each call looks up that array's device address
+ * (cudaGetSymbolAddress) in the current context.  Runs on the current
+ * device, on `stream` (NULL: the legacy default stream), and is synchronous:
+ * it returns once *count is written, so it must not be called while
+ * `stream`, or any stream in global capture mode, is being captured.  Every
+ * call shares the array, which keeps the previous call's contents (the
+ * counters are cleared at the start of each call): calls that overlap on the
+ * GPU race. */
 pc_status pc_tc_count_noalloc(const uint64_t* d_vlist, const int32_t* d_elist, uint64_t n, uint64_t m,
                               void* stream, uint64_t* count);
 

@@ -10,14 +10,17 @@
 // carries (each GPU that loads libpc.so holds it until the process exits).
 //
 // The array holds the per-vertex prefix lengths |N(u) & [0,u)| for at most
-// kNoAllocMaxVertices vertices plus two counters, so graphs with more
-// vertices are rejected.  All calls share it and it keeps the previous call's
-// contents: each call clears the counters before use, and two calls whose
-// work overlaps on the GPU (different streams, no ordering between them)
-// race on it.
-#include <climits>
-#include <mutex>
-
+// kNoAllocMaxVertices vertices plus the total, the pivot counter and an error
+// word, so graphs with more vertices are rejected.  All calls share it and it
+// keeps the previous call's contents: each call clears the counters and the
+// error word before use and writes dplus for its own n vertices only, and two
+// calls whose work overlaps on the GPU (different streams, no ordering
+// between them) race on it.
+//
+// The CSR is checked as far as memory safety needs: offsets must be
+// non-decreasing and end at m, and every neighbour id that is dereferenced
+// must lie in [0, n).  A violation sets the error word, the counting kernel
+// does no work, and the call returns PC_ERR_INVALID_INPUT.
 #include "pc_internal.cuh"
 #include "tc_kernels.cuh"
 
@@ -27,24 +30,36 @@ namespace na {
 constexpr uint64_t kNoAllocMaxVertices = 1ull << 20;
 constexpr int kWarps = 8;
 
-// [0, kNoAllocMaxVertices): dplus; then the triangle total and the pivot counter.
+// [0, kNoAllocMaxVertices): dplus; then the triangle total, the error word
+// (adjacent, so one 16-byte copy returns both) and the pivot counter.
 struct NoAllocScratch {
     uint32_t dplus[kNoAllocMaxVertices];
     unsigned long long total;
+    unsigned long long error;  // 1: offsets not monotone / not ending at m; 2: neighbour id outside [0, n)
     unsigned long long next_pivot;
 };
 
 static __device__ __align__(256) NoAllocScratch g_scratch;
 
+// Zeroes the total, the pivot counter and the error word (one thread, first
+// launch of every call, so nothing a previous call left behind is read).
+__global__ void k_na_clear(NoAllocScratch* __restrict__ s) {
+    s->total = 0;
+    s->error = 0;
+    s->next_pivot = 0;
+}
+
+// dplus of every row, and the offset checks; it only ever sets the error word.
 __global__ void k_na_prepare(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj, uint64_t n,
-                             NoAllocScratch* __restrict__ s) {
+                             uint64_t m, NoAllocScratch* __restrict__ s) {
     const uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (u == 0) {
-        s->total = 0;
-        s->next_pivot = 0;
-    }
     if (u >= n) return;
     uint64_t lo = off[u], hi = off[u + 1];
+    if (lo > hi || hi > m || (u + 1 == n && hi != m)) {
+        s->dplus[u] = 0;
+        atomicOr(&s->error, 1ull);
+        return;
+    }
     const uint64_t b = lo;
     while (lo < hi) {
         const uint64_t mid = (lo + hi) >> 1;
@@ -62,6 +77,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_na_tc(const uint64_t* __restric
                                                        NoAllocScratch* __restrict__ s) {
     using namespace tc;
     __shared__ int32_t table[kWarps][kHashSlots];
+    // every block reads the prepare kernel's verdict before any row access
+    // (stream order makes it visible); the counting is skipped on a bad CSR
+    if (*(volatile unsigned long long*)&s->error) return;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int32_t* T = table[w];
     for (int i = lane; i < kHashSlots; i += 32) T[i] = -1;
@@ -86,6 +104,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_na_tc(const uint64_t* __restric
             __syncwarp();
             for (uint64_t e = rb + dp + lane; e < re; e += 32) {
                 const int32_t c = adj[e];
+                if ((uint64_t)(uint32_t)c >= n) {
+                    atomicOr(&s->error, 2ull);
+                    continue;
+                }
                 const int32_t* row = adj + off[c];
                 const uint32_t lim = s->dplus[c];
                 for (uint32_t i = 0; i < lim; ++i) {
@@ -105,6 +127,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_na_tc(const uint64_t* __restric
         } else {
             for (uint64_t e = rb + dp + lane; e < re; e += 32) {
                 const int32_t c = adj[e];
+                if ((uint64_t)(uint32_t)c >= n) {
+                    atomicOr(&s->error, 2ull);
+                    continue;
+                }
                 cnt += merge_below(adj + off[c], s->dplus[c], nb, dp, b);
             }
         }
@@ -113,19 +139,14 @@ __global__ void __launch_bounds__(kWarps * 32) k_na_tc(const uint64_t* __restric
     if (lane == 0 && cnt) atomicAdd(&s->total, cnt);
 }
 
-// Device address of g_scratch per device, resolved once with that device current.
-static std::mutex g_mu;
-static NoAllocScratch* g_addr[64];
-
-static pc_status scratch_address(int device, NoAllocScratch** out) {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (device < 0 || device >= 64) return fail(PC_ERR_INVALID_INPUT, "device index out of range");
-    if (!g_addr[device]) {
-        void* p = nullptr;
-        PC_CUDA(cudaGetSymbolAddress(&p, g_scratch));
-        g_addr[device] = static_cast<NoAllocScratch*>(p);
-    }
-    *out = g_addr[device];
+// Device address of g_scratch in the caller's current context.  It is looked
+// up on every call (a cheap query that allocates nothing): a cached address
+// would go stale after cudaDeviceReset or under another context made current
+// by a driver-API caller, and the kernels would then write through it.
+static pc_status scratch_address(NoAllocScratch** out) {
+    void* p = nullptr;
+    PC_CUDA(cudaGetSymbolAddress(&p, g_scratch));
+    *out = static_cast<NoAllocScratch*>(p);
     return PC_OK;
 }
 
@@ -152,16 +173,20 @@ pc_status pc_tc_count_noalloc(const uint64_t* d_vlist, const int32_t* d_elist, u
     int device = 0;
     PC_CUDA(cudaGetDevice(&device));
     NoAllocScratch* s = nullptr;
-    PC_TRY(scratch_address(device, &s));
+    PC_TRY(scratch_address(&s));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    k_na_prepare<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(d_vlist, d_elist, n, s);
+    k_na_clear<<<1, 1, 0, st>>>(s);
+    PC_LAUNCHED();
+    k_na_prepare<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(d_vlist, d_elist, n, m, s);
     PC_LAUNCHED();
     k_na_tc<<<(unsigned)(sm_count(device) * 8), kWarps * 32, 0, st>>>(d_vlist, d_elist, n, s);
     PC_LAUNCHED();
-    unsigned long long total = 0;
-    PC_CUDA(cudaMemcpyAsync(&total, &s->total, sizeof(total), cudaMemcpyDeviceToHost, st));
+    unsigned long long res[2] = {0, 0};  // total, error
+    PC_CUDA(cudaMemcpyAsync(res, &s->total, sizeof(res), cudaMemcpyDeviceToHost, st));
     PC_CUDA(cudaStreamSynchronize(st));
-    *count = total;
+    if (res[1] & 1ull) return fail(PC_ERR_INVALID_INPUT, "CSR offsets are not non-decreasing or do not end at m");
+    if (res[1] & 2ull) return fail(PC_ERR_INVALID_INPUT, "CSR holds a neighbour id outside [0, n)");
+    *count = res[0];
     return PC_OK;
 }
 
