@@ -6,21 +6,33 @@ edge factor 16, seed 1, degree-relabelled, 1024 equal-vertex partitions.
 A step is one Partitioned_Graph::solve_triangle_counting_merge over the whole
 graph.  Rank 0 prints one JSON line.
 
- * value   -- GTEPS = undirected edges / device time of one step, graph
-              resident in HBM (CUDA events on the library's stream), with the
-              learned per-partition selector (PC_VARIANT_AUTO).
- * e2e     -- the same through the C ABI from pinned host buffers: CSR upload
-              (validated), partition view, plan, counting, 8-byte result read.
- * roofline -- the algorithmic bytes of the merge formulation of triangle
-              counting, B = 4 W + 12 |E+| + 8 (n+1) with W = sum over oriented
-              edges of (d+(u) + d+(v)), over the summed duration of the
-              counting kernels, against the measured HBM copy bandwidth
-              (MEASURED_PEAKS.json; the 6650 GB/s fallback when it is absent).
+ * value    -- GTEPS = undirected edges / device time of one step, graph
+               resident in HBM (CUDA events on the library's stream), with the
+               learned per-partition selector (PC_VARIANT_AUTO).
+ * e2e      -- the same through the C ABI from pinned host buffers: CSR upload
+               (validated), partition view, plan, counting, 8-byte result read.
+ * roofline -- the algorithmic bytes of the pivot form the kernels run,
+               B = 8 (n+1) + 4 m (the CSR) + 4 n (the prefix lengths d+)
+               + 12 |E+| (per in-edge c -> b: the in-neighbour's offset and
+               prefix length) + 4 * wedges (every in-neighbour's prefix below
+               its pivot, wedges = sum_c C(d+(c), 2)), over the summed device
+               time of the counting kernels, against the measured HBM copy
+               bandwidth (MEASURED_PEAKS.json; the 6650 GB/s fallback when it
+               is absent).  The merge formulation's read volume over the same
+               time is reported beside it as an effective rate.
+ * parity   -- the oracle's count of the same arrays on all host cores, and
+               the pinned count of this graph (tests/golden/pinned_counts.json,
+               matched by the CSR's fingerprint); a mismatch fails the run.
  * cpu_baseline -- the reference's own loop (Graph::solve_triangle_counting_merge,
-              src/Graph.cpp:358-365, calling Graph::cnt_common_neis_less_than_merge)
-              over an every-k-th-row sample on all host cores, extrapolated.
+               src/Graph.cpp:358-365, calling Graph::cnt_common_neis_less_than_merge,
+               compiled from its sources into oracle/_ref) over a row sample on
+               all host cores: GTEPS = oriented edges of the sampled rows / time.
 With N > 1 (torchrun) every rank runs an independent replica on its own GPU
 (the path does not shard: replicas only); value = all ranks' edges / max time.
+
+--impl reference times that reference loop alone, on the same graph built by
+the oracle's generator (no part of the product library is loaded), one row
+sample per step.
 """
 from __future__ import annotations
 
@@ -61,6 +73,8 @@ def parse():
                     help="many-graph workload: 4096 RMAT graphs (scale 10..16, ef 8..32, seeds 0..4095), "
                          "TC + LCC + BFS in one persistent launch")
     ap.add_argument("--batch-graphs", type=int, default=4096)
+    ap.add_argument("--batch-check-graphs", type=int, default=64,
+                    help="graphs whose LCC and BFS are checked and whose reference time is the CPU baseline")
     ap.add_argument("--suite", default="",
                     help="comma list of per-config suites: algos (RMAT-22, P=256, all nine algorithms with full-size "
                          "parity against the reference on the host cores), skew (ER and Chung-Lu, n=2^24, m=2^28, "
@@ -114,24 +128,30 @@ class Dist:
 
 # ---- workload -------------------------------------------------------------------
 
-def make_graph(pc, scale, ef, seed, device=False):
-    """The seeded RMAT graph: generated and built on the GPU (pc_graph_rmat)
-    for our arm, by the host generator (the same arrays) for the reference
-    arm, which runs none of the library's GPU code."""
+WORKLOAD_GRAPH = "RMAT(0.57,0.19,0.19,0.05) scale {scale} ef {ef} seed {seed}, symmetrised, deduplicated, " \
+                 "degree-relabelled"
+PINNED = ROOT / "tests" / "golden" / "pinned_counts.json"
+
+
+def workload_config(args, n, m):
+    """The config block both arms print (identical keys and values)."""
+    return {"workload": f"tc_rmat{args.scale}_ef{args.edge_factor}_p{args.partitions}",
+            "graph": WORKLOAD_GRAPH.format(scale=args.scale, ef=args.edge_factor, seed=args.seed),
+            "n": int(n), "m_directed": int(m), "undirected_edges": int(m // 2), "partitions": args.partitions,
+            "l2": "inputs larger than L2 (CSR %.2f GB)" % ((8 * (n + 1) + 4 * m) / 1e9)}
+
+
+def make_graph(pc, scale, ef, seed):
+    """The seeded RMAT graph, generated and built on the GPU (pc_graph_rmat)."""
     t = time.time()
-    if device:
-        g = pc.Graph.rmat_device(scale, ef, seed)
-        vl, el = g.get_csr_vlist(), g.get_csr_elist()
-        g.close()
-    else:
-        vl, el, _ = pc.HostCSR.rmat(scale, ef, seed).arrays()
+    g = pc.Graph.rmat_device(scale, ef, seed)
+    vl, el = g.get_csr_vlist(), g.get_csr_elist()
+    g.close()
     return vl, el, time.time() - t
 
 
-def tc_algorithmic_bytes(vl, el, chunk_rows=1 << 20):
-    """B_TC = 4 W + 12 |E+| + 8 (n+1), W = sum over oriented edges (u -> v, v < u)
-    of d+(u) + d+(v) with d+(x) = |N(x) & [0, x)| (the merge read volume).
-    Computed in row chunks to bound host memory."""
+def oriented_prefix_lengths(vl, el, chunk_rows=1 << 20):
+    """d+(u) = |N(u) & [0, u)| for every row, in row chunks to bound host memory."""
     n = vl.size - 1
     deg = np.diff(vl).astype(np.int64)
     dplus = np.zeros(n, np.int64)
@@ -140,6 +160,22 @@ def tc_algorithmic_bytes(vl, el, chunk_rows=1 << 20):
         rows = np.repeat(np.arange(lo, hi, dtype=np.int64), deg[lo:hi])
         seg = el[vl[lo]:vl[hi]]
         dplus[lo:hi] = np.bincount(rows[seg < rows] - lo, minlength=hi - lo)
+    return dplus
+
+
+def tc_bytes(vl, el, chunk_rows=1 << 20):
+    """Algorithmic bytes of one triangle count.
+
+    pivot: 8 (n+1) + 4 m + 4 n + 12 |E+| + 4 wedges -- the form the kernels
+        run (each triangle a < b < c found at pivot b from in-neighbour c
+        while scanning N(c) & [0, b); the scan of c for pivot b reads b's rank
+        in N+(c) ids, so the scans add up to sum_c C(d+(c), 2) = the wedges).
+    merge: 4 W + 12 |E+| + 8 (n+1), W = sum over oriented edges (u -> v, v < u)
+        of d+(u) + d+(v) -- the reference's merge formulation, whose read
+        volume is the unit of the effective rate."""
+    n, m = vl.size - 1, el.size
+    dplus = oriented_prefix_lengths(vl, el, chunk_rows)
+    deg = np.diff(vl).astype(np.int64)
     W = int((dplus * dplus).sum())
     for lo in range(0, n, chunk_rows):
         hi = min(n, lo + chunk_rows)
@@ -147,7 +183,47 @@ def tc_algorithmic_bytes(vl, el, chunk_rows=1 << 20):
         seg = el[vl[lo]:vl[hi]]
         W += int(dplus[seg[seg < rows]].sum())
     e_plus = int(dplus.sum())
-    return 4 * W + 12 * e_plus + 8 * (n + 1), W, e_plus
+    wedges = int((dplus * (dplus - 1) // 2).sum())
+    return {"pivot_bytes": 8 * (n + 1) + 4 * m + 4 * n + 12 * e_plus + 4 * wedges, "wedges": wedges,
+            "merge_bytes": 4 * W + 12 * e_plus + 8 * (n + 1), "W": W, "e_plus": e_plus}
+
+
+def csr_fingerprint(vl, el):
+    """The fingerprint tests/golden/make_pinned.py records for each graph."""
+    k = np.arange(el.size, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        f_el = int(np.sum(el.astype(np.uint64) * (k * np.uint64(0x9E3779B97F4A7C15) + np.uint64(1)),
+                          dtype=np.uint64))
+        f_vl = int(np.sum(vl.astype(np.uint64) * np.uint64(0xBF58476D1CE4E5B9), dtype=np.uint64))
+    return {"n": int(vl.size - 1), "m": int(el.size), "fp_elist": f_el, "fp_vlist": f_vl}
+
+
+def pinned_count(vl, el):
+    """(name, T) of the pinned graph with this CSR's fingerprint, else (None, None)."""
+    try:
+        data = json.loads(PINNED.read_text())
+    except Exception:
+        return None, None
+    fp = csr_fingerprint(vl, el)
+    for name, rec in data.items():
+        if all(rec.get(k) == v for k, v in fp.items()):
+            return name, int(rec["T"])
+    return None, None
+
+
+def tc_parity(O, vl, el, T, threads):
+    """The oracle's count of the same arrays (all host threads, dynamic
+    schedule) and the pinned count; raises SystemExit on any mismatch."""
+    t = time.perf_counter()
+    t_oracle = O.tc_merge(vl, el)
+    dt = time.perf_counter() - t
+    name, t_pinned = pinned_count(vl, el)
+    rec = {"gpu_T": int(T), "oracle_T": int(t_oracle), "oracle_s": round(dt, 1), "oracle_threads": threads,
+           "pinned": name, "pinned_T": t_pinned}
+    rec["match"] = bool(t_oracle == T and (t_pinned is None or t_pinned == T))
+    if not rec["match"]:
+        raise SystemExit(f"triangle count mismatch: {rec}")
+    return rec
 
 
 def hbm_peak():
@@ -212,64 +288,86 @@ class ClockSampler:
 
 # ---- the reference arm ----------------------------------------------------------
 
-def reference_tc_sample(vl, el, target_s, threads, graph=None):
-    """Times the reference's TC loop on every k-th row; returns (GTEPS, sample)."""
-    from oracle import oracle as O
-    n = vl.size - 1
-    e_plus = el.size // 2
-    if O.Reference.available():
-        R = O.Reference(vl, el, threads=threads)
-        run = R.tc_rows
-        kind = "reference"
-    else:
-        R = None
-        run = lambda rows: O.tc_rows(vl, el, rows)  # noqa: E731
-        kind = "port"
-    k = 4096
-    while True:
-        rows = np.arange(0, n, k, dtype=np.int32)
+class ReferenceSample:
+    """The reference's TC loop (body and static OpenMP schedule of
+    Graph::solve_triangle_counting_merge, src/Graph.cpp:358-365, compiled from
+    its sources into oracle/_ref) over the rows u = 0 mod k of a graph; k is
+    chosen so that one pass takes about target_s seconds on `threads` host
+    threads.  The rate is the oriented edges of the sampled rows over the
+    measured time of the pass: nothing is extrapolated."""
+
+    def __init__(self, O, vl, el, target_s, threads, dplus=None):
+        self.n = vl.size - 1
+        self.threads = threads
+        if O.Reference.available():
+            self.R = O.Reference(vl, el, threads=threads)
+            self.run = self.R.tc_rows
+            self.kind = "reference"
+        else:
+            self.R = None
+            self.run = lambda rows: O.tc_rows(vl, el, rows)  # noqa: E731
+            self.kind = "port"
+        if dplus is None:
+            dplus = oriented_prefix_lengths(vl, el)
+        k = 4096
+        while True:
+            rows = np.arange(0, self.n, k, dtype=np.int32)
+            t = time.perf_counter()
+            self.run(rows)
+            dt = time.perf_counter() - t
+            if dt * 4 >= target_s or k == 1:
+                break
+            k = max(1, int(k * max(dt, 1e-3) / target_s * 1.5)) if dt > 0.05 else max(1, k // 16)
+        self.k, self.rows = k, rows
+        self.edges = int(dplus[rows.astype(np.int64)].sum())
+
+    def time_pass(self):
         t = time.perf_counter()
-        run(rows)
-        dt = time.perf_counter() - t
-        if dt * 4 >= target_s or k == 1:
-            break
-        k = max(1, int(k * max(dt, 1e-3) / target_s * 1.5)) if dt > 0.05 else max(1, k // 16)
-    gteps = e_plus / (dt * k) / 1e9
-    sample = (f"the reference's TC loop (body and static OpenMP schedule of Graph::solve_triangle_counting_merge) "
-              f"over rows u = 0 mod {k} ({rows.size} of {n} rows) of the {graph or f'RMAT-{int(np.log2(n))}'} graph, "
-              f"{dt:.2f} s, extrapolated x{k}")
-    return gteps, kind, sample, R, run, rows, k, e_plus
+        self.run(self.rows)
+        return time.perf_counter() - t
+
+    def describe(self, seconds, graph):
+        return (f"the reference's TC loop (body and static OpenMP schedule of Graph::solve_triangle_counting_merge) "
+                f"over rows u = 0 mod {self.k} ({self.rows.size} of {self.n} rows, {self.edges} oriented edges) of "
+                f"the {graph} graph, {seconds:.2f} s per pass on {self.threads} threads; "
+                f"GTEPS = those edges / that time")
+
+    def close(self):
+        if self.R is not None:
+            self.R.close()
 
 
 def run_reference_arm(args, dist):
-    import partitionandconquer_b200 as pc
-    vl, el, _ = make_graph(pc, args.scale, args.edge_factor, args.seed)
+    """One row-sample pass of the reference's loop per step; the graph comes
+    from the oracle's generator, so no part of the product library loads."""
+    from oracle import oracle as O
+    t0 = time.time()
+    vl, el = O.gen_rmat(args.scale, args.edge_factor, args.seed)
+    t_gen = time.time() - t0
     threads = os.cpu_count() or 1
-    gteps, kind, sample, R, run, rows, k, e_plus = reference_tc_sample(vl, el, args.cpu_sample_seconds, threads)
+    per_step = min(args.cpu_sample_seconds, max(1.0, 150.0 / max(1, args.steps + args.warmup)))
+    S = ReferenceSample(O, vl, el, per_step, threads)
     for _ in range(args.warmup):
-        run(rows)
-    times = []
-    for _ in range(args.steps):
-        t = time.perf_counter()
-        run(rows)
-        times.append(time.perf_counter() - t)
-    step_s = statistics.median(times) * k
-    value = e_plus / step_s / 1e9
+        S.time_pass()
+    times = [S.time_pass() for _ in range(args.steps)]
+    step_s = statistics.median(times)
+    value = S.edges / step_s / 1e9
+    graph = f"RMAT-{args.scale}"
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "GTEPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_s * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-        "data": "synthetic (seeded RMAT)",
-        "config": {"workload": f"tc_rmat{args.scale}_ef{args.edge_factor}_p{args.partitions}", "partitions": args.partitions,
-                   "path": "Graph::solve_triangle_counting_merge loop (the partitioned constructor needs P*n "
-                           "offsets plus 2*P*n vectors: infeasible in memory at this size)"},
-        "cpu_baseline": {"value": round(value, 6), "unit": "GTEPS", "cores": threads, "kind": kind,
-                         "sample": sample},
+        "data": "synthetic (seeded RMAT, built by the oracle's generator)",
+        "config": workload_config(args, vl.size - 1, el.size),
+        "path": "Graph::solve_triangle_counting_merge loop on a row sample per step (the partitioned constructor "
+                "needs P*n offsets plus 2*P*n vectors: infeasible in memory at this size)",
+        "cpu_baseline": {"value": round(value, 6), "unit": "GTEPS", "cores": threads, "kind": S.kind,
+                         "sample": S.describe(step_s, graph)},
         "e2e": {"value": round(value, 6), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "setup": {"graph_gen_s": round(t_gen, 1)},
     }
     print(json.dumps(line), flush=True)
-    if R is not None:
-        R.close()
+    S.close()
 
 
 # ---- our arm ------------------------------------------------------------------------
@@ -324,6 +422,20 @@ def plan_bounds(pc, pg):
     return out
 
 
+def traffic_per_count(tb):
+    """DRAM bytes (read + write) of one count, from the ncu capture recorded in
+    profiles/tc_dram_traffic.txt: `dram_bytes_per_pivot_byte=` is the captured
+    count's DRAM bytes over its pivot-form algorithmic bytes, which scales the
+    capture to this graph; None when no capture is recorded."""
+    tf = ROOT / "profiles" / "tc_dram_traffic.txt"
+    if not tf.exists():
+        return None
+    for ln in tf.read_text().splitlines():
+        if ln.startswith("dram_bytes_per_pivot_byte="):
+            return round(float(ln.split("=", 1)[1]) * tb["pivot_bytes"])
+    return None
+
+
 def time_device(pc, torch, pg, stream, variant, steps, warmup):
     for _ in range(warmup):
         pg.triangle_count(variant=variant)
@@ -352,9 +464,10 @@ def run_ours(args, dist):
     _lib.check(_lib.lib.pc_set_device(dev))
     if dist.world > 1:
         os.environ.setdefault("OMP_NUM_THREADS", str(max(1, (os.cpu_count() or 1) // dist.world)))
-    vl, el, t_gen = make_graph(pc, args.scale, args.edge_factor, args.seed, device=True)
+    vl, el, t_gen = make_graph(pc, args.scale, args.edge_factor, args.seed)
     n = vl.size - 1
-    algo_bytes, W, e_plus = tc_algorithmic_bytes(vl, el)
+    tb = tc_bytes(vl, el)
+    e_plus = tb["e_plus"]
     v2p = pc.equal_vertex_partition(n, args.partitions)
     if args.profile:
         if args.heuristic:
@@ -397,13 +510,8 @@ def run_ours(args, dist):
     # roofline of the counting kernels (event-timed inside the call on the same stream)
     kernel_ms = statistics.median(k_learned)
     peak, peak_kind = hbm_peak()
-    achieved = algo_bytes / (kernel_ms / 1e3) / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / "tc_rmat24_traffic.txt"
-    if tf.exists():
-        for ln in tf.read_text().splitlines():
-            if ln.startswith("dram_bytes_per_call="):
-                traffic = float(ln.split("=", 1)[1])
+    achieved = tb["pivot_bytes"] / (kernel_ms / 1e3) / 1e9
+    traffic = traffic_per_count(tb)
 
     # end to end through the C ABI from pinned host buffers
     from partitionandconquer_b200 import _lib as L
@@ -436,31 +544,30 @@ def run_ours(args, dist):
     e2e_value = dist.world * e_plus / e2e_s / 1e9
     h2d = vl.nbytes + el.nbytes + v2p.nbytes
 
-    cpu = None
-    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        gteps, kind, sample, R, *_ = reference_tc_sample(vl, el, args.cpu_sample_seconds, os.cpu_count() or 1)
-        cpu = {"value": round(gteps, 6), "unit": "GTEPS", "cores": os.cpu_count() or 1, "kind": kind,
-               "sample": sample}
-        if R is not None:
-            R.close()
+    cpu, parity = None, None
+    if dist.rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        threads = os.cpu_count() or 1
+        parity = tc_parity(O, vl, el, T, threads)
+        if dist.world == 1:
+            S = ReferenceSample(O, vl, el, args.cpu_sample_seconds, threads)
+            dt = S.time_pass()
+            cpu = {"value": round(S.edges / dt / 1e9, 6), "unit": "GTEPS", "cores": threads, "kind": S.kind,
+                   "sample": S.describe(dt, f"RMAT-{args.scale}")}
+            S.close()
 
     if dist.rank == 0:
-        hist = list(st_learned.variant_hist)
         line = {
             "metric": METRIC, "value": round(value, 4), "unit": "GTEPS", "n_gpus": dist.world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms_max, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded RMAT, generated in-process)",
-            "config": {
-                "workload": f"tc_rmat{args.scale}_ef{args.edge_factor}_p{args.partitions}",
-                "graph": f"RMAT(0.57,0.19,0.19,0.05) scale {args.scale} ef {args.edge_factor} seed {args.seed}, "
-                         "symmetrised, deduplicated, degree-relabelled", "n": int(n), "m_directed": int(el.size),
-                "undirected_edges": int(e_plus), "partitions": args.partitions, "triangles": int(T),
-                "l2": "inputs larger than L2 (CSR %.2f GB)" % ((vl.nbytes + el.nbytes) / 1e9),
-                "selector": "learned (MLP judged by the autotuned heuristic)",
-                "parallelism": "replicas" if dist.world > 1 else "1 GPU",
-                "plan_variants_per_unit": hist,
-            },
+            "config": workload_config(args, n, el.size),
+            "parallelism": "replicas" if dist.world > 1 else "1 GPU",
+            "triangles": int(T),
+            "parity": parity,
+            "selector": "learned (MLP judged by the autotuned heuristic)",
+            "plan_variants_per_unit": list(st_learned.variant_hist),
             "learned_vs_plain": {"learned_ms": round(step_ms, 4), "plain_ms": round(plain_ms, 4),
                                  "speedup": round(plain_ms / step_ms, 4),
                                  "plain_variants_per_unit": list(st_plain.variant_hist),
@@ -471,7 +578,10 @@ def run_ours(args, dist):
                                           (round(statistics.median(x) * 1e3, 2) for x in zip(*phases))))},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
-                         "algorithmic_bytes": int(algo_bytes), "W": int(W), "kernel_ms": round(kernel_ms, 4)},
+                         "algorithmic_bytes": int(tb["pivot_bytes"]), "wedges": int(tb["wedges"]),
+                         "kernel_ms": round(kernel_ms, 4),
+                         "effective_merge_gbs": round(tb["merge_bytes"] / (kernel_ms / 1e3) / 1e9, 1),
+                         "merge_bytes": int(tb["merge_bytes"]), "W": int(tb["W"])},
             "cpu_baseline": cpu,
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
@@ -485,7 +595,12 @@ def run_ours(args, dist):
 def run_batch(args):
     """Config 4: TC + LCC + BFS for every graph of the arena in one
     persistent-kernel launch replayed from a captured CUDA graph, schedule
-    from the autotuner.  value = undirected edges of all graphs / launch time."""
+    from the autotuner.  value = undirected edges of all graphs / launch time.
+    Every graph's triangle count is checked against the oracle, LCC and BFS on
+    a sample of graphs; the CPU baseline is the reference's own per-graph
+    calls (Graph::solve_triangle_counting_merge, solve_lcc_merge, solve_bfs,
+    src/Graph.cpp:355-368, 814-840, 621-646) run one graph after another on a
+    sample of graphs."""
     import torch
 
     import partitionandconquer_b200 as pc
@@ -507,23 +622,45 @@ def run_batch(args):
             times.append(r["ms"])
     ms = statistics.median(times)
     e_plus = el.size // 2
-    # verify a stratified sample of graphs against the oracle
+    # every graph's triangle count against the oracle
+    t = time.perf_counter()
+    bad_tc = []
+    for g in range(G):
+        v0, v1 = int(voff[g]), int(voff[g + 1])
+        sv = (vl[v0:v1 + 1] - vl[v0]).astype(np.uint64)
+        se = (el[vl[v0]:vl[v1]] - v0).astype(np.int32)
+        if O.tc_merge(sv, se) != int(r["tc"][g]):
+            bad_tc.append(g)
+    t_tc_check = time.perf_counter() - t
+    if bad_tc:
+        raise SystemExit(f"batch triangle counts differ from the oracle on graphs {bad_tc[:10]}")
+    # LCC and BFS on a sample; the reference's per-graph calls timed on the same sample
     rng = np.random.default_rng(0)
-    sample = sorted(set(rng.choice(G, size=min(G, 24), replace=False).tolist()))
-    cpu_s = 0.0
+    sample = sorted(set(rng.choice(G, size=min(G, args.batch_check_graphs), replace=False).tolist()))
+    cpu_s, cpu_kind, threads = 0.0, "reference" if O.Reference.available() else "port", os.cpu_count() or 1
     for g in sample:
         v0, v1 = int(voff[g]), int(voff[g + 1])
         sv = (vl[v0:v1 + 1] - vl[v0]).astype(np.uint64)
         se = (el[vl[v0]:vl[v1]] - v0).astype(np.int32)
-        t = time.perf_counter()
-        tc = O.tc_merge(sv, se)
-        lcc = O.lcc(sv, se)
-        bfs = O.bfs(sv, se, 0)
-        cpu_s += time.perf_counter() - t
-        bad = [name for name, ok in (("tc", tc == int(r["tc"][g])), ("bfs", np.array_equal(bfs, r["bfs"][v0:v1])),
+        lcc, bfs = O.lcc(sv, se), O.bfs(sv, se, 0)
+        bad = [name for name, ok in (("bfs", np.array_equal(bfs, r["bfs"][v0:v1])),
                                      ("lcc", np.array_equal(lcc, r["lcc"][v0:v1], equal_nan=True))) if not ok]
         if bad:
             raise SystemExit(f"batch result mismatch on graph {g}: {bad}")
+        if cpu_kind == "reference":
+            R = O.Reference(sv, se, threads=threads)
+            t = time.perf_counter()
+            R.tc()
+            R.lcc()
+            R.bfs_parents(0)
+            cpu_s += time.perf_counter() - t
+            R.close()
+        else:
+            t = time.perf_counter()
+            O.tc_merge(sv, se)
+            O.lcc(sv, se)
+            O.bfs(sv, se, 0)
+            cpu_s += time.perf_counter() - t
     sample_edges = sum(int(vl[voff[g + 1]] - vl[voff[g]]) // 2 for g in sample)
     line = {
         "metric": "batched TC+LCC+BFS over 4096 RMAT graphs (undirected edges per second)", "value":
@@ -533,9 +670,16 @@ def run_batch(args):
         "config": {"workload": f"batch{G}_rmat10-16_ef8-32", "graphs": G, "n": int(vl.size - 1),
                    "m_directed": int(el.size), "tasks": "TC+LCC+BFS", "schedule": tuned,
                    "launch": "one persistent kernel per step, replayed CUDA graph"},
-        "verified_graphs": len(sample),
-        "cpu_baseline": {"value": round(sample_edges / cpu_s / 1e9, 6), "unit": "GTEPS", "cores": os.cpu_count(),
-                         "kind": "port", "sample": f"oracle TC+LCC+BFS on {len(sample)} sampled graphs, {cpu_s:.1f} s"},
+        "graphs_per_s": round(G / (ms / 1e3), 1),
+        "parity": {"tc_graphs_checked": G, "tc_match": True, "tc_check_s": round(t_tc_check, 1),
+                   "lcc_bfs_graphs_checked": len(sample), "lcc_bfs_match": True},
+        "cpu_baseline": {"value": round(sample_edges / cpu_s / 1e9, 6), "unit": "GTEPS", "cores": threads,
+                         "kind": cpu_kind, "graphs_per_s": round(len(sample) / cpu_s, 2),
+                         "sample": f"the reference's Graph::solve_triangle_counting_merge + solve_lcc_merge + "
+                                   f"solve_bfs, one graph after another, on {len(sample)} sampled graphs "
+                                   f"({sample_edges} undirected edges), {cpu_s:.1f} s"
+                         if cpu_kind == "reference" else f"oracle TC+LCC+BFS on {len(sample)} sampled graphs, "
+                                                         f"{cpu_s:.1f} s"},
         "clocks": clocks.summary(), "setup": {"graph_gen_s": round(t_gen, 1)},
     }
     print(json.dumps(line), flush=True)
@@ -576,8 +720,9 @@ def _rel_ok(a, b, tol):
 
 
 def _edge_sum_bytes(vl, el):
-    """SURVEY-style algorithmic bytes of the per-edge intersection sweep:
-    4 * sum over CSR entries (d(u) + d(v)) + 12 m + 8 (n + 1)."""
+    """Algorithmic bytes of the per-edge intersection sweep (a merge of N(u)
+    and N(v) for every CSR entry): 4 * sum over entries (d(u) + d(v)) + 12 m
+    + 8 (n + 1)."""
     deg = np.diff(vl).astype(np.int64)
     s = int((deg * deg).sum()) + int(deg[el].sum())
     return 4 * s + 12 * el.size + 8 * deg.size + 8
@@ -599,7 +744,7 @@ def suite_algos(pc, O, args, emit):
     peak, peak_kind = hbm_peak()
     lab0 = np.arange(n, dtype=np.int32)
     prio = pc.vertex_priority(args.seed, n)
-    tc_bytes = tc_algorithmic_bytes(vl, el)[0]
+    b_tc = tc_bytes(vl, el)["pivot_bytes"]
     es_bytes = _edge_sum_bytes(vl, el)
     sweep = 4 * m + 8 * (n + 1) + 4 * n
     import torch
@@ -616,8 +761,8 @@ def suite_algos(pc, O, args, emit):
         # name, gpu call, cpu (kind, call), units, bytes, compare
         # the reference's own TC and LCC loops take minutes here (static OpenMP schedule over
         # degree-sorted rows: 91 s for TC on 16 cores); the oracle (dynamic schedule) checks them
-        ("tc", lambda: pg.triangle_count(), ("port", lambda: O.tc_merge(vl, el)), m // 2, tc_bytes, "exact"),
-        ("tc_galloping", lambda: pg.solve_triangle_counting_galloping(), None, m // 2, tc_bytes, "exact6"),
+        ("tc", lambda: pg.triangle_count(), ("port", lambda: O.tc_merge(vl, el)), m // 2, b_tc, "exact"),
+        ("tc_galloping", lambda: pg.solve_triangle_counting_galloping(), None, m // 2, b_tc, "exact6"),
         ("lcc", lambda: pg.solve_lcc_merge(out=o_lcc), ("port", lambda: O.lcc(vl, el)), m, es_bytes, 1e-6),
         ("jaccard_edges", lambda: pg.jaccard_edges(out=o_jac), ("port", lambda: O.jaccard_edges(vl, el)), m, es_bytes, 1e-6),
         ("bfs", lambda: pg.solve_bfs(0, out=o_bfs), ("port", lambda: O.bfs(vl, el, 0)), m, sweep, "exact"),
@@ -683,10 +828,41 @@ def _learned_vs_plain(pc, torch, pg, stream, steps, warmup):
             "learned_variants": list(stl.variant_hist), "plain_variants": list(stp.variant_hist)}
 
 
+def jaccard_parity(O, vl, el, jac, T, full_limit=1e11, sample_rows=20000):
+    """All-edge Jaccard against the oracle.  Graphs whose merge sweep
+    (sum over entries of d(u) + d(v)) is at most full_limit ids are compared
+    entry by entry with the oracle's full result.  Larger ones are audited in
+    full -- every entry round-trips to an integer count, equals its twin, and
+    the counts add up to 6 T with T the oracle's triangle count -- and compared
+    exactly on an evenly spaced sample of rows."""
+    deg = np.diff(vl).astype(np.int64)
+    sweep = int((deg * deg).sum())
+    t = time.perf_counter()
+    if sweep <= full_limit:
+        want = O.jaccard_edges(vl, el)
+        bad = int(np.count_nonzero(want.view(np.uint32) != jac.view(np.uint32)))
+        rec = {"jaccard_check": "full", "jaccard_mismatches": bad}
+    else:
+        sum_c, bad_rt, bad_twin = O.jaccard_audit(vl, el, jac)
+        n = vl.size - 1
+        rows = np.arange(0, n, max(1, n // sample_rows), dtype=np.int32)
+        want = O.jaccard_rows(vl, el, rows)
+        got = np.concatenate([jac[vl[r]:vl[r + 1]] for r in rows])
+        bad = int(np.count_nonzero(want.view(np.uint32) != got.view(np.uint32)))
+        rec = {"jaccard_check": f"audit (sum of counts = 6 T, round-trip, twins) + exact on {rows.size} rows "
+                                f"({want.size} entries)",
+               "jaccard_sum_counts": sum_c, "six_T": 6 * int(T), "jaccard_roundtrip_bad": bad_rt,
+               "jaccard_twin_bad": bad_twin, "jaccard_mismatches": bad}
+        bad += bad_rt + bad_twin + int(sum_c != 6 * int(T))
+    rec["jaccard_check_s"] = round(time.perf_counter() - t, 1)
+    rec["jaccard_match"] = bad == 0
+    return rec
+
+
 def suite_selector_graph(pc, O, torch, args, emit, name, h, P, suite):
     vl, el, _ = h.arrays()
     n, m = vl.size - 1, el.size
-    algo_bytes, W, e_plus = tc_algorithmic_bytes(vl, el)
+    tb = tc_bytes(vl, el)
     g = pc.Graph(vlist=vl, elist=el)
     pg = pc.Partitioned_Graph(g, pc.equal_vertex_partition(n, P))
     stream = torch.cuda.ExternalStream(g.stream())
@@ -695,36 +871,36 @@ def suite_selector_graph(pc, O, torch, args, emit, name, h, P, suite):
     peak, peak_kind = hbm_peak()
     kms = lp["learned_ms"]
     # all-edge Jaccard runs the triangle kernels in per-edge mode under the
-    # same plan: learned (selector on) and plain (selector off), same output
-    t_j, jac = _timed(lambda: pg.jaccard_edges(), max(1, args.steps // 2), 1)
+    # same plan: learned (selector on) and plain (selector off), same output,
+    # written into a caller-owned pinned buffer (the copy back is a DMA of m floats)
+    jac = torch.empty(m, dtype=torch.float32, pin_memory=True).numpy()
+    jac_p = torch.empty(m, dtype=torch.float32, pin_memory=True).numpy()
+    t_j, _ = _timed(lambda: pg.jaccard_edges(out=jac), max(1, args.steps // 2), 1)
     pc.selector.enable(False)
     try:
-        t_jp, jac_p = _timed(lambda: pg.jaccard_edges(), max(1, args.steps // 2), 1)
+        t_jp, _ = _timed(lambda: pg.jaccard_edges(out=jac_p), max(1, args.steps // 2), 1)
     finally:
         pc.selector.enable(True)
-    if not np.array_equal(jac, jac_p):
+    if not np.array_equal(jac.view(np.uint32), jac_p.view(np.uint32)):
         raise SystemExit("Jaccard differs between the learned and the plain plan")
-    # Jaccard spot check: the oracle's formula on a sample of rows
-    rows = np.arange(0, n, max(1, n // 500), dtype=np.int64)
-    bad = 0
-    deg = np.diff(vl).astype(np.int64)
-    for u in rows[:500]:
-        nu = el[vl[u]:vl[u + 1]]
-        for k, v in enumerate(nu[:16]):
-            c = np.intersect1d(nu, el[vl[v]:vl[v + 1]], assume_unique=True).size
-            want = np.float32(c / (deg[u] + deg[v] - c))
-            if jac[vl[u] + k] != want:
-                bad += 1
-    gteps_cpu, kind, sample, Rf, *_ = reference_tc_sample(vl, el, args.cpu_sample_seconds, os.cpu_count() or 1, name)
-    if Rf is not None:
-        Rf.close()
-    emit({"suite": suite, "workload": f"{name}_p{P}", "n": int(n), "m_directed": int(m), **lp,
-          "tc_gteps_learned": round(e_plus / (kms / 1e3) / 1e9, 4),
-          "tc_roofline_frac": round(algo_bytes / (kms / 1e3) / 1e9 / peak, 4), "peak_kind": peak_kind,
-          "W": int(W), "jaccard_ms": round(t_j * 1e3, 3), "jaccard_plain_ms": round(t_jp * 1e3, 3),
-          "jaccard_speedup": round(t_jp / t_j, 4), "jaccard_gteps": round(m / t_j / 1e9, 4),
-          "jaccard_spot_mismatches": bad,
-          "cpu_tc_gteps": gteps_cpu, "cpu_kind": kind, "cpu_cores": os.cpu_count(), "cpu_sample": sample})
+    rec = {"suite": suite, "workload": f"{name}_p{P}", "n": int(n), "m_directed": int(m), **lp,
+           "tc_gteps_learned": round(tb["e_plus"] / (kms / 1e3) / 1e9, 4),
+           "tc_roofline_frac": round(tb["pivot_bytes"] / (kms / 1e3) / 1e9 / peak, 4), "peak_kind": peak_kind,
+           "wedges": tb["wedges"], "jaccard_ms": round(t_j * 1e3, 3), "jaccard_plain_ms": round(t_jp * 1e3, 3),
+           "jaccard_speedup": round(t_jp / t_j, 4), "jaccard_gteps": round(m / t_j / 1e9, 4),
+           "jaccard_result": "caller-owned pinned host array (the call includes the copy of m floats)"}
+    if not args.profile:
+        threads = os.cpu_count() or 1
+        rec["parity"] = tc_parity(O, vl, el, lp["triangles"], threads)
+        rec.update(jaccard_parity(O, vl, el, jac, lp["triangles"]))
+        S = ReferenceSample(O, vl, el, args.cpu_sample_seconds, threads)
+        dt = S.time_pass()
+        rec.update({"cpu_tc_gteps": round(S.edges / dt / 1e9, 6), "cpu_kind": S.kind, "cpu_cores": threads,
+                    "cpu_sample": S.describe(dt, name)})
+        S.close()
+    emit(rec)
+    if not args.profile and not rec["jaccard_match"]:
+        raise SystemExit(f"Jaccard mismatch on {name}")
     pg.close()
     g.close()
 

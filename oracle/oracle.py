@@ -20,7 +20,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle.so"
 REF_SO = HERE / "_ref" / "libpcref.so"
-REF_SRC = Path(os.environ.get("PC_REFERENCE_DIR", "/root/reference"))
+# the reference checkout: PC_REFERENCE_DIR, else `reference` beside the repository
+REF_SRC = Path(os.environ.get("PC_REFERENCE_DIR", str(HERE.parent.parent / "reference")))
 
 P = C.c_void_p
 i32, u64, f32, f64 = C.c_int32, C.c_uint64, C.c_float, C.c_double
@@ -70,6 +71,8 @@ def _load_c():
         "or_lcc": (None, [u64, P, P, P]),
         "or_jaccard_edges": (None, [u64, P, P, P]),
         "or_jaccard_queries": (None, [u64, P, P, P, i32, P]),
+        "or_jaccard_rows": (None, [u64, P, P, P, u64, P]),
+        "or_jaccard_audit": (None, [u64, P, P, P, P, P, P]),
         "or_batch_pairs": (None, [u64, P, P, P, u64, P]),
         "or_batch_sets": (None, [u64, P, P, P, P, u64, P]),
         "or_bfs": (None, [u64, P, P, i32, P]),
@@ -81,6 +84,14 @@ def _load_c():
         "or_cdlp": (None, [u64, P, P, i32, P]),
         "or_friend_triangle": (u64, [u64, P, P, i32, P, u64]),
         "or_square_count": (u64, [u64, P, P]),
+        "og_rmat": (P, [C.c_uint32, u64, u64, C.c_int]),
+        "og_er": (P, [C.c_uint32, u64, u64, C.c_int]),
+        "og_chung_lu": (P, [C.c_uint32, u64, f64, u64, u64, C.c_int]),
+        "og_rmat_batch": (P, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, u64, P]),
+        "og_n": (u64, [P]),
+        "og_m": (u64, [P]),
+        "og_copy": (None, [P, P, P]),
+        "og_free": (None, [P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -103,6 +114,40 @@ def _csr(vl, el):
     vl = np.ascontiguousarray(vl, np.uint64)
     el = np.ascontiguousarray(el, np.int32)
     return vl, el, vl.size - 1
+
+
+# ---- seeded graphs (pc_graphgen.c) -------------------------------------------------
+
+def _take(h):
+    if not h:
+        raise MemoryError("graph generation failed")
+    lib = clib()
+    n, m = int(lib.og_n(h)), int(lib.og_m(h))
+    vl = np.empty(n + 1, np.uint64)
+    el = np.empty(m, np.int32)
+    lib.og_copy(h, _ptr(vl), _ptr(el))
+    lib.og_free(h)
+    return vl, el
+
+
+def gen_rmat(scale, edge_factor, seed, relabel=True):
+    """RMAT(0.57, 0.19, 0.19, 0.05) with 2^scale vertices and 2^scale *
+    edge_factor draws, symmetrised, deduplicated, degree-relabelled."""
+    return _take(clib().og_rmat(scale, edge_factor, seed, int(relabel)))
+
+
+def gen_er(scale, nedges, seed, relabel=True):
+    return _take(clib().og_er(scale, nedges, seed, int(relabel)))
+
+
+def gen_chung_lu(scale, nedges, beta, dmax, seed, relabel=True):
+    return _take(clib().og_chung_lu(scale, nedges, beta, dmax, seed, int(relabel)))
+
+
+def gen_rmat_batch(G, smin, smax, emin, emax, seed=0):
+    voff = np.empty(G + 1, np.uint64)
+    vl, el = _take(clib().og_rmat_batch(G, smin, smax, emin, emax, seed, _ptr(voff)))
+    return vl, el, voff
 
 
 # ---- the C restatement ---------------------------------------------------------
@@ -164,6 +209,28 @@ def jaccard_edges(vl, el):
     out = np.empty(el.size, np.float32)
     clib().or_jaccard_edges(n, _ptr(vl), _ptr(el), _ptr(out))
     return out
+
+
+def jaccard_rows(vl, el, rows):
+    """Exact all-edge Jaccard values of the listed rows, concatenated."""
+    vl, el, n = _csr(vl, el)
+    r = np.ascontiguousarray(rows, np.int32)
+    d = (vl[r.astype(np.int64) + 1] - vl[r.astype(np.int64)]).astype(np.int64)
+    out = np.empty(int(d.sum()), np.float32)
+    clib().or_jaccard_rows(n, _ptr(vl), _ptr(el), _ptr(r), r.size, _ptr(out))
+    return out
+
+
+def jaccard_audit(vl, el, J):
+    """(sum of recovered common-neighbour counts (= 6 T), entries that do not
+    round-trip, entries whose twin differs) for an all-edge Jaccard result."""
+    vl, el, n = _csr(vl, el)
+    J = np.ascontiguousarray(J, np.float32)
+    if J.size != el.size:
+        raise ValueError("one Jaccard value per CSR entry expected")
+    res = [C.c_uint64() for _ in range(3)]
+    clib().or_jaccard_audit(n, _ptr(vl), _ptr(el), _ptr(J), *(C.byref(x) for x in res))
+    return tuple(int(x.value) for x in res)
 
 
 def jaccard_queries(vl, el, q):

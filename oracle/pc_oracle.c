@@ -223,6 +223,64 @@ void or_jaccard_edges(uint64_t n, const uint64_t* vl, const int32_t* el, float* 
     }
 }
 
+/* or_jaccard_edges restricted to the rows listed (a bounded exact sample of a
+ * graph too large for the full sweep): out holds, row after row in the order
+ * given, one value per entry of each row. */
+void or_jaccard_rows(uint64_t n, const uint64_t* vl, const int32_t* el, const int32_t* rows, uint64_t nrows,
+                     float* out) {
+    (void)n;
+    uint64_t* base = malloc((nrows + 1) * sizeof(uint64_t));
+    base[0] = 0;
+    for (uint64_t i = 0; i < nrows; i++) base[i + 1] = base[i] + (vl[rows[i] + 1] - vl[rows[i]]);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t i = 0; i < (int64_t)nrows; i++) {
+        int64_t u = rows[i];
+        uint64_t du = vl[u + 1] - vl[u];
+        for (uint64_t j = vl[u]; j < vl[u + 1]; j++) {
+            int32_t v = el[j];
+            uint64_t dv = vl[v + 1] - vl[v];
+            double c = (double)merge_cnt(vl, el, u, v);
+            out[base[i] + (j - vl[u])] = (float)(c / ((double)(du + dv) - c));
+        }
+    }
+    free(base);
+}
+
+/* A size-independent audit of an all-edge Jaccard result J[m] (the
+ * Graph::solve_jsim_merge formula per CSR entry, stored as float).  Per entry
+ * (u, v) with D = d(u) + d(v), the common-neighbour count c is recovered as
+ * round(J D / (1 + J)), and the entry must round-trip: (float)(c / (D - c))
+ * == J bit for bit (adjacent c give distinct floats while D < 2^24).  The
+ * twin entry (v, u), found by binary search in N(v), must hold the same
+ * value.  *sum_c is the sum of c over all entries, which is 6 T for a graph
+ * with T triangles (each triangle lies on three edges, each stored twice). */
+void or_jaccard_audit(uint64_t n, const uint64_t* vl, const int32_t* el, const float* J, uint64_t* sum_c,
+                      uint64_t* bad_roundtrip, uint64_t* bad_twin) {
+    uint64_t sc = 0, br = 0, bt = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : sc, br, bt)
+    for (int64_t u = 0; u < (int64_t)n; u++) {
+        uint64_t du = vl[u + 1] - vl[u];
+        for (uint64_t j = vl[u]; j < vl[u + 1]; j++) {
+            int32_t v = el[j];
+            uint64_t D = du + (vl[v + 1] - vl[v]);
+            double x = (double)J[j];
+            double cr = x * (double)D / (1.0 + x);
+            int64_t c = (int64_t)(cr + 0.5);
+            if (c < 0 || (uint64_t)c > D / 2 || (float)((double)c / ((double)D - (double)c)) != J[j]) br++;
+            else sc += (uint64_t)c;
+            uint64_t lo = vl[v], hi = vl[v + 1];
+            while (lo < hi) {
+                uint64_t mid = (lo + hi) >> 1;
+                if (el[mid] < (int32_t)u) lo = mid + 1; else hi = mid;
+            }
+            if (lo == vl[v + 1] || el[lo] != (int32_t)u || J[lo] != J[j]) bt++;
+        }
+    }
+    *sum_c = sc;
+    *bad_roundtrip = br;
+    *bad_twin = bt;
+}
+
 /* Graph::solve_jsim_merge (src/Graph.cpp:798-812). */
 void or_jaccard_queries(uint64_t n, const uint64_t* vl, const int32_t* el, const int32_t* q, int32_t nq, double* out) {
     (void)n;

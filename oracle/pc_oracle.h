@@ -18,6 +18,10 @@ int or_layout(uint64_t n, const uint64_t* vl, const int32_t* el, const int32_t* 
 uint64_t or_tc_partitioned(uint64_t n, const uint64_t* pvl, const int32_t* pel, int32_t P);
 void or_lcc(uint64_t n, const uint64_t* vl, const int32_t* el, double* out);
 void or_jaccard_edges(uint64_t n, const uint64_t* vl, const int32_t* el, float* out);
+void or_jaccard_rows(uint64_t n, const uint64_t* vl, const int32_t* el, const int32_t* rows, uint64_t nrows,
+                     float* out);
+void or_jaccard_audit(uint64_t n, const uint64_t* vl, const int32_t* el, const float* J, uint64_t* sum_c,
+                      uint64_t* bad_roundtrip, uint64_t* bad_twin);
 void or_jaccard_queries(uint64_t n, const uint64_t* vl, const int32_t* el, const int32_t* q, int32_t nq, double* out);
 void or_batch_pairs(uint64_t n, const uint64_t* vl, const int32_t* el, const int32_t* pairs, uint64_t nq, uint64_t* out);
 void or_batch_sets(uint64_t n, const uint64_t* vl, const int32_t* el, const int32_t* ids, const uint64_t* offs,

@@ -186,3 +186,55 @@ def test_partitioned_jaccard_defect_is_documented(O):
         assert np.all(part >= 1.0)  # a count, not a ratio
     finally:
         R.close()
+
+
+@pytest.mark.parametrize("case", ["rmat", "rmat_raw", "er", "chung_lu", "batch"])
+def test_oracle_generator_equals_product_generator(pc, O, case):
+    """The oracle's generator (used where the product library must not load:
+    the benchmark's reference arm, the pinned-count script) builds the same
+    arrays as the product's host generator."""
+    if case == "rmat":
+        a, b = O.gen_rmat(13, 16, 2), pc.HostCSR.rmat(13, 16, 2).arrays()
+    elif case == "rmat_raw":
+        a, b = O.gen_rmat(11, 8, 5, relabel=False), pc.HostCSR.rmat(11, 8, 5, relabel=False).arrays()
+    elif case == "er":
+        a, b = O.gen_er(12, 50000, 7), pc.HostCSR.er(12, 50000, 7).arrays()
+    elif case == "chung_lu":
+        a, b = O.gen_chung_lu(12, 50000, 2.1, 1024, 3), pc.HostCSR.chung_lu(12, 50000, 2.1, 1024, 3).arrays()
+    else:
+        vl, el, voff = O.gen_rmat_batch(9, 6, 9, 8, 16, 0)
+        h, voff2 = pc.HostCSR.rmat_batch(9, 6, 9, 8, 16, seed=0)
+        np.testing.assert_array_equal(voff, voff2)
+        a, b = (vl, el), h.arrays()
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+
+
+def test_jaccard_audit_and_rows(O):
+    vl, el = O.gen_rmat(11, 16, 4)
+    J = O.jaccard_edges(vl, el)
+    T = O.tc_merge(vl, el)
+    assert O.jaccard_audit(vl, el, J) == (6 * T, 0, 0)
+    rows = np.arange(3, vl.size - 1, 5, dtype=np.int32)
+    want = np.concatenate([J[vl[r]:vl[r + 1]] for r in rows])
+    np.testing.assert_array_equal(O.jaccard_rows(vl, el, rows), want)
+    # a planted one-ulp error in the oracle's own output is caught twice
+    k = int(np.flatnonzero(J > 0)[0])
+    bad = J.copy()
+    bad[k] = np.nextafter(bad[k], np.float32(1))
+    s, rt, tw = O.jaccard_audit(vl, el, bad)
+    assert rt == 1 and tw == 2 and s != 6 * T
+
+
+def test_pinned_counts_are_consistent():
+    """The pinned file's counts: oracle and reference agree wherever both ran,
+    and config 1's graph gives the reference's known 15,643,386 triangles."""
+    import json
+
+    from conftest import GOLDEN
+    data = json.loads((GOLDEN / "pinned_counts.json").read_text())
+    assert data["rmat16_ef16_s1"]["T"] == 15643386
+    for name, rec in data.items():
+        assert rec["T"] == rec["T_oracle"], name
+        if "T_reference" in rec:
+            assert rec["T_reference"] == rec["T"], name
