@@ -767,6 +767,8 @@ def suite_algos(pc, O, args, emit):
         ("jaccard_edges", lambda: pg.jaccard_edges(out=o_jac), ("port", lambda: O.jaccard_edges(vl, el)), m, es_bytes, 1e-6),
         ("bfs", lambda: pg.solve_bfs(0, out=o_bfs), ("port", lambda: O.bfs(vl, el, 0)), m, sweep, "exact"),
         ("sssp", lambda: pg.solve_sssp(0, out=o_sssp), ("port", lambda: O.sssp(vl, el, w, 0)), m, sweep, "exact"),
+        ("sssp_bellman_ford", lambda: pg.solve_sssp(0, out=o_sssp, method=pc.SSSP_BELLMAN_FORD),
+         ("port", lambda: O.sssp(vl, el, w, 0)), m, sweep, "exact"),
         ("pagerank_fp32", lambda: pg.page_rank(0.85, 20, out=o_pr), ("port", lambda: O.pagerank_f64(vl, el, 0.85, 20)),
          m * 20, 20 * (8 * m + 20 * n), 1e-6),
         ("pagerank_fp64", lambda: pg.page_rank(0.85, 20, fp64=True, out=o_pr64),

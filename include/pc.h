@@ -231,8 +231,23 @@ pc_status pc_square_count(pc_pgraph* pg, uint64_t* out);
 pc_status pc_bfs(pc_pgraph* pg, int32_t src, int32_t* rank);
 /* Partitioned_Graph::solve_sssp (src/Graph.cpp:2263-2309) / Graph::solve_sssp
  * (src/Graph.cpp:842-868): exact distances with the int32 weights,
- * unreached = INT32_MAX / 2.  Requires a weighted graph. */
+ * unreached = INT32_MAX / 2.  Requires a weighted graph.  pc_sssp is
+ * pc_sssp_ex(PC_SSSP_AUTO, delta 0). */
 pc_status pc_sssp(pc_pgraph* pg, int32_t src, int32_t* dist);
+/* The schedule of the relaxations, which never changes the result (both are
+ * label-correcting and end at the exact distances):
+ *   PC_SSSP_BELLMAN_FORD   frontier Bellman-Ford, the reference's partitioned
+ *                          schedule (src/Graph.cpp:2263-2309): every improved
+ *                          vertex is relaxed in the next round;
+ *   PC_SSSP_DELTA_STEPPING delta-stepping (near/far piles): only vertices whose
+ *                          distance is below the current bucket bound are
+ *                          relaxed; buckets are `delta` wide (0: 32 x mean
+ *                          weight / mean degree, computed on the device);
+ *   PC_SSSP_AUTO           delta-stepping with delta chosen from the graph. */
+#define PC_SSSP_AUTO 0
+#define PC_SSSP_BELLMAN_FORD 1
+#define PC_SSSP_DELTA_STEPPING 2
+pc_status pc_sssp_ex(pc_pgraph* pg, int32_t src, int32_t method, int32_t delta, int32_t* dist);
 /* Partitioned_Graph::page_rank (src/Graph.cpp:1555-1602): x0 = d/(damping n),
  * x[v] <- (1-damping)/n + sum_{u in N(v)} x[u] * damping / d(u), in fp32.
  * init != NULL starts from the caller's vector instead, which is

@@ -32,6 +32,9 @@ def device_count() -> int:
     return int(lib.pc_device_count())
 
 
+SSSP_AUTO, SSSP_BELLMAN_FORD, SSSP_DELTA_STEPPING = 0, 1, 2
+
+
 def launch_count() -> int:
     """Kernels launched by libpc.so in this process."""
     return int(lib.pc_launch_count())
@@ -532,9 +535,11 @@ class Partitioned_Graph:
         check(lib.pc_bfs(self._pg, u, ptr(out)))
         return out
 
-    def solve_sssp(self, src: int, out=None):
+    def solve_sssp(self, src: int, out=None, method: int = 0, delta: int = 0):
+        """Exact distances from src.  method: SSSP_AUTO (0), SSSP_BELLMAN_FORD (1)
+        or SSSP_DELTA_STEPPING (2) with bucket width `delta` (0: from the graph)."""
         out = _result(out, self.get_vertex_num(), np.int32)
-        check(lib.pc_sssp(self._pg, src, ptr(out)))
+        check(lib.pc_sssp_ex(self._pg, src, method, delta, ptr(out)))
         return out
 
     def page_rank(self, damping_factor: float = 0.85, num_iterations: int = 20, init=None, fp64: bool = False,

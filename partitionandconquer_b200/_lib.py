@@ -114,6 +114,7 @@ _SIG = {
     "pc_batch_count_sets": (i32, [P, P, P, u64, P]),
     "pc_bfs": (i32, [P, i32, P]),
     "pc_sssp": (i32, [P, i32, P]),
+    "pc_sssp_ex": (i32, [P, i32, i32, i32, P]),
     "pc_pagerank": (i32, [P, f32, i32, P, P]),
     "pc_pagerank_f64": (i32, [P, f64, i32, P, P]),
     "pc_kcore": (i32, [P, P, P]),

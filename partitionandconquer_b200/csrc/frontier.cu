@@ -213,12 +213,45 @@ __global__ void k_bfs_finish(const int32_t* __restrict__ dist, uint64_t n, int32
     if (i < n) rank[i] = dist[i] == 0 ? -1 : dist[i];
 }
 
-// ---- SSSP (frontier Bellman-Ford) --------------------------------------------
+// ---- SSSP: frontier Bellman-Ford and delta-stepping --------------------------
+//
+// Both forms relax the rows of a frontier with atomicMin and queue every
+// vertex whose distance falls; they differ in which improved vertices are
+// relaxed next.  Bellman-Ford (kDelta = false) relaxes all of them in the
+// next round.  Delta-stepping (kDelta = true; Meyer and Sanders, "Delta-
+// stepping: a parallelizable shortest path algorithm", J. Algorithms 2003, in
+// the near/far-pile form of Davidson, Baxter, Garland and Owens, IPDPS 2014)
+// relaxes only vertices whose new distance is below the current bucket's
+// upper bound `thr` ("near"); the others go to a far pile that is split when
+// the bucket is exhausted.  Both are label-correcting: every improvement is
+// queued, so both end at the exact shortest distances (integer weights >= 0).
+struct SsspPush {
+    int32_t thr;                 // delta-stepping: near bound (exclusive)
+    int32_t* __restrict__ far;   // far pile and its length
+    uint32_t* __restrict__ farn;
+    int32_t* __restrict__ farflag;  // 1 while the vertex is in the far pile
+};
 
+template <bool kDelta>
+__device__ __forceinline__ void sssp_relax_edge(int32_t du, int32_t v, int32_t wt, int32_t* __restrict__ dist,
+                                                int32_t* __restrict__ flag, const SsspPush& P, bool* near,
+                                                bool* far) {
+    const int32_t nd = du + wt;
+    if (nd < dist[v]) {
+        const int32_t old = atomicMin(&dist[v], nd);
+        if (nd < old) {
+            if (!kDelta || nd < P.thr) *near = atomicExch(&flag[v], 1) == 0;
+            else *far = atomicExch(&P.farflag[v], 1) == 0;
+        }
+    }
+}
+
+template <bool kDelta>
 __global__ void k_sssp_relax(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
                              const int32_t* __restrict__ w, const int32_t* __restrict__ fq, uint32_t fn,
                              int32_t* __restrict__ dist, int32_t* __restrict__ flag, int32_t* __restrict__ nq,
-                             uint32_t* __restrict__ nn, int32_t* __restrict__ hq, uint32_t* __restrict__ hn) {
+                             uint32_t* __restrict__ nn, int32_t* __restrict__ hq, uint32_t* __restrict__ hn,
+                             SsspPush P) {
     const int lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -232,17 +265,14 @@ __global__ void k_sssp_relax(const uint64_t* __restrict__ off, const int32_t* __
         const int32_t du = dist[u];
         for (uint64_t j0 = b; j0 < e; j0 += 32) {
             const uint64_t j = j0 + lane;
-            bool push = false;
+            bool near = false, far = false;
             int32_t v = 0;
             if (j < e) {
                 v = adj[j];
-                const int32_t nd = du + w[j];
-                if (nd < dist[v]) {
-                    const int32_t old = atomicMin(&dist[v], nd);
-                    if (nd < old) push = atomicExch(&flag[v], 1) == 0;
-                }
+                sssp_relax_edge<kDelta>(du, v, w[j], dist, flag, P, &near, &far);
             }
-            warp_append(push, v, nq, nn);
+            warp_append(near, v, nq, nn);
+            if (kDelta) warp_append(far, v, P.far, P.farn);
         }
     }
 }
@@ -250,23 +280,70 @@ __global__ void k_sssp_relax(const uint64_t* __restrict__ off, const int32_t* __
 // The heavy frontier vertices of a relaxation round, spread over the grid.
 // dist[u] may fall further while its row is being relaxed; any value read is
 // an achieved distance, and a vertex whose distance falls is queued again.
+template <bool kDelta>
 __global__ void k_sssp_relax_heavy(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
                                    const int32_t* __restrict__ w, const int32_t* __restrict__ hq,
                                    const uint32_t* __restrict__ hn, int32_t* __restrict__ dist,
-                                   int32_t* __restrict__ flag, int32_t* __restrict__ nq, uint32_t* __restrict__ nn) {
+                                   int32_t* __restrict__ flag, int32_t* __restrict__ nq, uint32_t* __restrict__ nn,
+                                   SsspPush P) {
     heavy_rows(off, hq, *hn, [&](int32_t u, uint64_t j, bool ok) {
-        bool push = false;
+        bool near = false, far = false;
         int32_t v = 0;
         if (ok) {
             v = adj[j];
-            const int32_t nd = dist[u] + w[j];
-            if (nd < dist[v]) {
-                const int32_t old = atomicMin(&dist[v], nd);
-                if (nd < old) push = atomicExch(&flag[v], 1) == 0;
+            sssp_relax_edge<kDelta>(dist[u], v, w[j], dist, flag, P, &near, &far);
+        }
+        warp_append(near, v, nq, nn);
+        if (kDelta) warp_append(far, v, P.far, P.farn);
+    });
+}
+
+// Smallest current distance in the far pile (entries at or above lo; lower
+// ones were relaxed in an earlier bucket), so empty buckets are skipped.
+__global__ void k_sssp_far_min(const int32_t* __restrict__ far, uint32_t fn, const int32_t* __restrict__ dist,
+                               int32_t lo, int32_t* __restrict__ out) {
+    int32_t mn = INT_MAX;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < fn; i += gridDim.x * blockDim.x) {
+        const int32_t d = dist[far[i]];
+        if (d >= lo) mn = min(mn, d);
+    }
+    for (int o = 16; o; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    if ((threadIdx.x & 31) == 0 && mn != INT_MAX) atomicMin(out, mn);
+}
+
+// Splits the far pile at the new bucket [lo, hi): entries whose distance
+// fell below lo were relaxed when it fell and are dropped; entries in
+// [lo, hi) become the near frontier; the rest stay in the far pile.
+__global__ void k_sssp_far_split(const int32_t* __restrict__ far, uint32_t fn, const int32_t* __restrict__ dist,
+                                 int32_t lo, int32_t hi, int32_t* __restrict__ flag, int32_t* __restrict__ farflag,
+                                 int32_t* __restrict__ nq, uint32_t* __restrict__ nn, int32_t* __restrict__ far2,
+                                 uint32_t* __restrict__ far2n) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t nr = (fn + 31) & ~31u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += stride) {
+        bool near = false, keep = false;
+        int32_t v = 0;
+        if (i < fn) {
+            v = far[i];
+            const int32_t d = dist[v];
+            keep = d >= hi;
+            if (!keep) {
+                farflag[v] = 0;
+                near = d >= lo && atomicExch(&flag[v], 1) == 0;
             }
         }
-        warp_append(push, v, nq, nn);
-    });
+        warp_append(near, v, nq, nn);
+        warp_append(keep, v, far2, far2n);
+    }
+}
+
+// Sum of m int32 values (non-negative weights) into *out.
+__global__ void k_sum_i32(const int32_t* __restrict__ a, uint64_t m, unsigned long long* __restrict__ out) {
+    unsigned long long x = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
+        x += (unsigned long long)(uint32_t)a[i];
+    x = warp_sum_u64(x);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(out, x);
 }
 
 __global__ void k_clear_flags(const int32_t* __restrict__ q, uint32_t qn, int32_t* __restrict__ flag) {
@@ -959,48 +1036,128 @@ pc_status pc_bfs(pc_pgraph* pg, int32_t src, int32_t* rank) {
 }
 
 pc_status pc_sssp(pc_pgraph* pg, int32_t src, int32_t* dist_host) {
+    return pc_sssp_ex(pg, src, PC_SSSP_AUTO, 0, dist_host);
+}
+
+pc_status pc_sssp_ex(pc_pgraph* pg, int32_t src, int32_t method, int32_t delta, int32_t* dist_host) {
     clear_error();
     if (!pg || !dist_host) return fail(PC_ERR_INVALID_INPUT, "null argument");
-    const uint64_t n = pg->g->n;
+    const uint64_t n = pg->g->n, m = pg->g->m;
     if (!pg->w) return fail(PC_ERR_INVALID_INPUT, "SSSP needs a weighted graph");
     if (src < 0 || (uint64_t)src >= n) return fail(PC_ERR_INVALID_INPUT, "source vertex out of range");
+    if (method != PC_SSSP_AUTO && method != PC_SSSP_BELLMAN_FORD && method != PC_SSSP_DELTA_STEPPING)
+        return fail(PC_ERR_INVALID_INPUT, "unknown SSSP method");
+    if (delta < 0) return fail(PC_ERR_INVALID_INPUT, "delta must be >= 0 (0: chosen from the graph)");
     PC_TRY(use_device(pg->g));
+    const bool use_delta = method != PC_SSSP_BELLMAN_FORD;
     const int32_t isrc = to_internal_id(pg, src);
     cudaStream_t s = pg->g->stream;
-    const uint64_t hcap = heavy_cap(n, pg->g->m);
-    PC_TRY(scratch_reserve(pg, n * 4 * 5 + hcap * 4 + 256));
+    const uint64_t hcap = heavy_cap(n, m);
+    PC_TRY(scratch_reserve(pg, n * 4 * (use_delta ? 9 : 5) + hcap * 4 + 1024));
     int32_t* dist = pg->scratch.take<int32_t>(n);
     int32_t* flag = pg->scratch.take<int32_t>(n);
     int32_t* q0 = pg->scratch.take<int32_t>(n);
     int32_t* q1 = pg->scratch.take<int32_t>(n);
     int32_t* out = pg->scratch.take<int32_t>(n);
     int32_t* hq = pg->scratch.take<int32_t>(hcap);
-    uint32_t* cnt = pg->scratch.take<uint32_t>(4);  // [0] next frontier, [1] heavy list
-    if (!cnt) return fail(PC_ERR_OOM, "SSSP scratch plan exceeds its reservation");
+    uint32_t* cnt = pg->scratch.take<uint32_t>(8);  // [0] next frontier, [1] heavy list, [2] far, [3] far', [4] min
+    int32_t *farflag = nullptr, *far0 = nullptr, *far1 = nullptr;
+    unsigned long long* wsum = nullptr;
+    if (use_delta) {
+        farflag = pg->scratch.take<int32_t>(n);
+        far0 = pg->scratch.take<int32_t>(n);
+        far1 = pg->scratch.take<int32_t>(n);
+        wsum = pg->scratch.take<unsigned long long>(1);
+    }
+    if (!cnt || (use_delta && !wsum)) return fail(PC_ERR_OOM, "SSSP scratch plan exceeds its reservation");
     const unsigned nb = (unsigned)ceil_div(n, kThreads);
     k_fill_i32<<<nb, kThreads, 0, s>>>(dist, n, INT_MAX / 2);  // src/test.cpp:202-203
     PC_LAUNCHED();
     PC_CUDA(cudaMemsetAsync(flag, 0, n * 4, s));
+    PC_CUDA(cudaMemsetAsync(cnt, 0, 32, s));
+    int32_t bucket = INT_MAX;  // Bellman-Ford: one unbounded bucket
+    if (use_delta) {
+        PC_CUDA(cudaMemsetAsync(farflag, 0, n * 4, s));
+        if (delta == 0) {
+            // Delta ~ 32 x mean weight / mean degree: about a warp's worth of
+            // improvements per vertex and bucket (Davidson et al.)
+            PC_CUDA(cudaMemsetAsync(wsum, 0, 8, s));
+            k_sum_i32<<<grid_for(pg), kThreads, 0, s>>>(pg->w, m, wsum);
+            PC_LAUNCHED();
+            unsigned long long h = 0;
+            PC_CUDA(cudaMemcpyAsync(&h, wsum, 8, cudaMemcpyDeviceToHost, s));
+            PC_TRY(sync(pg));
+            const double mean_w = m ? (double)h / (double)m : 1.0, mean_d = n ? (double)m / (double)n : 1.0;
+            delta = (int32_t)std::min<double>(1 << 30, std::max(1.0, std::round(32.0 * mean_w / std::max(1.0, mean_d))));
+        }
+        bucket = delta;
+    }
     const int32_t zero = 0;
     PC_CUDA(cudaMemcpyAsync(dist + isrc, &zero, 4, cudaMemcpyHostToDevice, s));
     PC_CUDA(cudaMemcpyAsync(q0, &isrc, 4, cudaMemcpyHostToDevice, s));
-    uint32_t fn = 1;
+    uint32_t fn = 1, farn = 0;
     int32_t* fq = q0;
     int32_t* nq = q1;
-    for (uint64_t round = 0; fn > 0; ++round) {
-        PC_CUDA(cudaMemsetAsync(cnt, 0, 8, s));
-        k_sssp_relax<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, pg->w, fq, fn, dist, flag, nq, cnt, hq,
-                                                       cnt + 1);
+    int32_t thr = bucket;
+    uint64_t rounds = 0;
+    const uint64_t round_cap = 4 * (n + 1) + 64;
+    for (;;) {
+        while (fn > 0) {
+            PC_CUDA(cudaMemsetAsync(cnt, 0, 8, s));
+            SsspPush P{thr, far0, cnt + 2, farflag};
+            if (use_delta) {
+                k_sssp_relax<true><<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, pg->w, fq, fn, dist, flag, nq,
+                                                                    cnt, hq, cnt + 1, P);
+                PC_LAUNCHED();
+                k_sssp_relax_heavy<true><<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, pg->w, hq, cnt + 1, dist,
+                                                                          flag, nq, cnt, P);
+            } else {
+                k_sssp_relax<false><<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, pg->w, fq, fn, dist, flag,
+                                                                     nq, cnt, hq, cnt + 1, P);
+                PC_LAUNCHED();
+                k_sssp_relax_heavy<false><<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, pg->w, hq, cnt + 1,
+                                                                           dist, flag, nq, cnt, P);
+            }
+            PC_LAUNCHED();
+            PC_TRY(read_u32(pg, cnt, &fn));
+            if (fn) {
+                k_clear_flags<<<(unsigned)ceil_div(fn, kThreads), kThreads, 0, s>>>(nq, fn, flag);
+                PC_LAUNCHED();
+            }
+            std::swap(fq, nq);
+            if (++rounds > round_cap) return fail(PC_ERR_TIMEOUT, "SSSP did not converge");
+        }
+        if (!use_delta) break;
+        PC_TRY(read_u32(pg, cnt + 2, &farn));
+        if (farn == 0) break;
+        // next bucket: from the smallest far distance at or above thr (the
+        // entries below thr were relaxed when their distance fell)
+        const int32_t big = INT_MAX;
+        PC_CUDA(cudaMemcpyAsync(cnt + 4, &big, 4, cudaMemcpyHostToDevice, s));
+        k_sssp_far_min<<<(unsigned)std::min<uint64_t>(ceil_div(farn, kThreads), 1024), kThreads, 0, s>>>(
+            far0, farn, dist, thr, reinterpret_cast<int32_t*>(cnt + 4));
         PC_LAUNCHED();
-        k_sssp_relax_heavy<<<grid_for(pg), kThreads, 0, s>>>(pg->off, pg->adj, pg->w, hq, cnt + 1, dist, flag, nq, cnt);
+        uint32_t mn_u = 0;
+        PC_TRY(read_u32(pg, cnt + 4, &mn_u));
+        const int32_t mn = (int32_t)mn_u;
+        const int32_t lo = thr;
+        const int32_t hi = mn == INT_MAX ? INT_MAX : (int32_t)std::min<int64_t>(INT_MAX, (int64_t)mn + delta);
+        PC_CUDA(cudaMemsetAsync(cnt, 0, 4, s));
+        PC_CUDA(cudaMemsetAsync(cnt + 3, 0, 4, s));
+        k_sssp_far_split<<<(unsigned)std::min<uint64_t>(ceil_div(farn, kThreads), 4096), kThreads, 0, s>>>(
+            far0, farn, dist, lo, hi, flag, farflag, fq, cnt, far1, cnt + 3);
         PC_LAUNCHED();
         PC_TRY(read_u32(pg, cnt, &fn));
+        PC_TRY(read_u32(pg, cnt + 3, &farn));
         if (fn) {
-            k_clear_flags<<<(unsigned)ceil_div(fn, kThreads), kThreads, 0, s>>>(nq, fn, flag);
+            k_clear_flags<<<(unsigned)ceil_div(fn, kThreads), kThreads, 0, s>>>(fq, fn, flag);
             PC_LAUNCHED();
         }
-        std::swap(fq, nq);
-        if (round > n + 1) return fail(PC_ERR_TIMEOUT, "SSSP did not converge");
+        std::swap(far0, far1);
+        PC_CUDA(cudaMemcpyAsync(cnt + 2, &farn, 4, cudaMemcpyHostToDevice, s));
+        thr = hi;
+        if (fn == 0 && farn == 0) break;
+        if (++rounds > round_cap) return fail(PC_ERR_TIMEOUT, "SSSP did not converge");
     }
     PC_TRY(gather_to_api_i32(pg, dist, out));
     PC_CUDA(cudaMemcpyAsync(dist_host, out, n * 4, cudaMemcpyDeviceToHost, s));

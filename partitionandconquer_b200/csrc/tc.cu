@@ -187,14 +187,14 @@ __global__ void k_item_fill(const uint64_t* __restrict__ off, const uint32_t* __
 
 // H[b - lo][a >> 5] |= bit(a) for a in N+(b), one warp per pivot.
 __global__ void k_matrix_rows(const uint64_t* __restrict__ off, const int32_t* __restrict__ adj,
-                              const uint32_t* __restrict__ dplus, int32_t lo, int32_t hi, uint32_t hwords,
+                              const uint32_t* __restrict__ dplus, int32_t lo, int32_t hi, uint32_t hstride,
                               uint32_t* __restrict__ H) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t b = lo + warp; b < hi; b += nwarps) {
         const int32_t* row = adj + off[b];
-        uint32_t* h = H + (uint64_t)(b - lo) * hwords;
+        uint32_t* h = H + (uint64_t)(b - lo) * hstride;
         for (uint32_t k = lane; k < dplus[b]; k += 32) {
             const int32_t a = row[k];
             atomicOr(&h[a >> 5], 1u << (a & 31));
@@ -202,32 +202,68 @@ __global__ void k_matrix_rows(const uint64_t* __restrict__ off, const int32_t* _
     }
 }
 
+// ---- asynchronous staging of an in-neighbour's span into shared memory ----
+//
+// cp.async (LDGSTS) copies 16-byte pieces global -> shared without passing
+// through registers; a lane waits for its own groups (wait_group), and a
+// __syncwarp() after the wait makes every lane's pieces visible to the warp.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// A warp-private stage holds up to kStageIds ids of a span: the copy starts
+// at the 16-byte boundary at or below the span (up to 3 ids early) and may
+// end up to 3 ids past it, which the 64 ids of padding after the last row
+// keep inside the adjacency array.
+constexpr uint32_t kStageIds = 512;
+constexpr uint32_t kStageVec = kStageIds / 4 + 1;  // uint4 per stage (span + up to 3 leading ids)
+
+// Issues the copies of ids [r, r + k) of adj into stage; returns the offset
+// of id r inside it, or -1 when the span does not fit (it is then read from
+// global memory).
+__device__ __forceinline__ int stage_span(const int32_t* __restrict__ adj, uint64_t r, uint32_t k, uint4* stage,
+                                          int lane) {
+    const uint32_t shift = (uint32_t)(r & 3);
+    const uint32_t nvec = (shift + k + 3) >> 2;
+    if (nvec > kStageVec) return -1;
+    const uint4* src = reinterpret_cast<const uint4*>(adj + (r - shift));
+    for (uint32_t x = lane; x < nvec; x += 32) cp_async16(stage + x, src + x);
+    return (int)shift;
+}
+
+// Word form of a block whose last pivot b sits at position jl: ceil(b/128)
+// 16-byte words per row against ceil(jl/32) probe rounds.
+__device__ __forceinline__ bool matrix_words_win(int32_t b, uint32_t jl) {
+    const uint32_t nv = ((((uint32_t)b + 31) >> 5) + 3) >> 2;
+    return ((nv + 31) >> 5) < ((jl + 31) >> 5);
+}
+
 // The pairs (b, c) of one in-neighbour c: S = N(c) & [0, min(hi, c)), pivots
-// at positions [j0, k).  Each pivot b = S[j] is taken by the whole warp:
-// j probes into row b (lanes read consecutive S[i], the probes hit one row)
-// or ceil(b/32) coalesced words of row b ANDed with the bitmap of S,
-// whichever is fewer.  The bitmap is built only when some pivot uses it.
-__device__ __forceinline__ unsigned long long matrix_pairs(const int32_t* __restrict__ S, uint32_t j0, uint32_t k,
-                                                           int32_t lo, uint32_t hwords,
-                                                           const uint32_t* __restrict__ H, uint32_t* Sb, int lane) {
+// at positions [j0, k).  Pivots are taken U consecutive positions at a time,
+// so each step of the warp has U independent row loads in flight per lane and
+// shares one load of S (or of its bitmap) between them:
+//  - probe form: lanes read S[i] for i below the block's last position and
+//    test bit S[i] of each pivot's row (i < j of that pivot);
+//  - word form: lanes AND 16-byte words of each row with the warp's
+//    shared-memory bitmap of S and count bits.  A row b has bits only below
+//    b, so words past a pivot's own length read zeros.
+// The form is chosen per block by the rounds each needs; the bitmap is built
+// only when some block uses it.  S may point to shared or global memory.
+template <int U>
+__device__ __forceinline__ unsigned long long matrix_block_pairs(const int32_t* S, uint32_t j0, uint32_t k,
+                                                                 int32_t lo, uint32_t hstride,
+                                                                 const uint32_t* __restrict__ H, uint32_t* Sb,
+                                                                 int lane) {
     unsigned long long cnt = 0;
-    // Pivots at positions j < 32 have fewer than 32 probes each: their pairs
-    // (j, i), i < j, are numbered f = j (j - 1) / 2 + i and taken 32 at a
-    // time, so every lane probes instead of j of them per pivot.
-    const uint32_t jm = k < 32u ? k : 32u;
-    if (j0 < jm) {
-        const uint32_t f1 = jm * (jm - 1) / 2;
-        for (uint32_t f = j0 * (j0 - 1) / 2 + lane; f < f1; f += 32) {
-            uint32_t j = (uint32_t)((1.0f + sqrtf(1.0f + 8.0f * (float)f)) * 0.5f);
-            while (j * (j - 1) / 2 > f) --j;
-            while ((j + 1) * j / 2 <= f) ++j;
-            const int32_t b = S[j], a = S[f - j * (j - 1) / 2];
-            cnt += (H[(uint64_t)(b - lo) * hwords + (a >> 5)] >> (a & 31)) & 1u;
-        }
-    }
-    const uint32_t jr = j0 > jm ? j0 : jm;  // the per-pivot loop starts here
     bool want = false;
-    for (uint32_t j = jr + lane; j < k; j += 32) want |= (uint32_t)((S[j] + 31) >> 5) <= j;
+    for (uint32_t jb = j0 + (uint32_t)lane * U; jb < k; jb += 32u * U) {
+        const uint32_t jl = min(jb + (uint32_t)U, k) - 1;
+        want |= matrix_words_win(S[jl], jl);
+    }
     const bool words = __any_sync(0xffffffffu, want);
     if (words) {
         for (uint32_t i = lane; i < k; i += 32) {
@@ -236,16 +272,35 @@ __device__ __forceinline__ unsigned long long matrix_pairs(const int32_t* __rest
         }
         __syncwarp();
     }
-    for (uint32_t j = jr; j < k; ++j) {
-        const int32_t b = S[j];
-        const uint32_t* h = H + (uint64_t)(b - lo) * hwords;
-        const uint32_t nw = (uint32_t)(b + 31) >> 5;
-        if (words && nw <= j) {
-            for (uint32_t x = lane; x < nw; x += 32) cnt += __popc(h[x] & Sb[x]);
+    const uint4* Sb4 = reinterpret_cast<const uint4*>(Sb);
+    for (uint32_t jb = j0; jb < k; jb += U) {
+        const uint32_t ju = min((uint32_t)U, k - jb), jl = jb + ju - 1;
+        const int32_t bl = S[jl];
+        const uint32_t* h[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int32_t b = (uint32_t)u < ju ? S[jb + u] : bl;
+            h[u] = H + (uint64_t)(b - lo) * hstride;
+        }
+        if (words && matrix_words_win(bl, jl)) {
+            const uint32_t nv = ((((uint32_t)bl + 31) >> 5) + 3) >> 2;
+            for (uint32_t x = lane; x < nv; x += 32) {
+                const uint4 sv = Sb4[x];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    if ((uint32_t)u < ju) {
+                        const uint4 v = __ldg(reinterpret_cast<const uint4*>(h[u]) + x);
+                        cnt += __popc(v.x & sv.x) + __popc(v.y & sv.y) + __popc(v.z & sv.z) + __popc(v.w & sv.w);
+                    }
+                }
+            }
         } else {
-            for (uint32_t i = lane; i < j; i += 32) {
+            for (uint32_t i = lane; i < jl; i += 32) {
                 const int32_t a = S[i];
-                cnt += (h[a >> 5] >> (a & 31)) & 1u;
+                const uint32_t w = (uint32_t)a >> 5, bit = (uint32_t)a & 31;
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if ((uint32_t)u < ju && i < jb + (uint32_t)u) cnt += (__ldg(h[u] + w) >> bit) & 1u;
             }
         }
     }
@@ -270,24 +325,29 @@ __device__ __forceinline__ void matrix_span(const uint64_t* __restrict__ off, co
 
 // In-neighbours c run in two phases.  The first kMatrixHeavy ids after lo
 // (the hubs, with the longest S_c) are taken one per warp from counter
-// next[0]; the rest 32 at a time from next[1], lanes locating the 32 spans
-// at once.  One-at-a-time for the hubs keeps a single warp from holding a
-// batch of 32 hubs at the end of the launch.
+// next[0], their spans read from global memory; the rest 32 at a time from
+// next[1], lanes locating the 32 spans at once.  In the second phase the
+// spans are staged into two warp-private shared-memory buffers by cp.async:
+// the next span's copies are in flight while the current one is counted.
+// One-at-a-time for the hubs keeps a single warp from holding a batch of 32
+// hubs at the end of the launch.
 constexpr uint64_t kMatrixHeavy = 65536;
 
+template <int U>
 __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t* __restrict__ off,
                                                                const int32_t* __restrict__ adj,
                                                                const uint32_t* __restrict__ dplus, int32_t lo,
-                                                               int32_t hi, uint64_t n, uint32_t hwords,
+                                                               int32_t hi, uint64_t n, uint32_t hstride,
                                                                const uint32_t* __restrict__ H,
                                                                unsigned long long* __restrict__ next,
                                                                unsigned long long* __restrict__ total,
                                                                unsigned long long* __restrict__ unit_cost,
                                                                int32_t unit) {
-    extern __shared__ uint32_t msm[];
+    extern __shared__ uint4 msm4[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    uint32_t* Sb = msm + (size_t)w * hwords;  // warp-private bitmap of S_c
-    for (uint32_t i = lane; i < hwords; i += 32) Sb[i] = 0;
+    uint32_t* Sb = reinterpret_cast<uint32_t*>(msm4) + (size_t)w * hstride;  // warp-private bitmap of S_c
+    uint4* stage = msm4 + (size_t)kMatrixWarps * (hstride / 4) + (size_t)w * 2 * kStageVec;
+    for (uint32_t i = lane; i < hstride; i += 32) Sb[i] = 0;
     __syncwarp();
     const long long t0 = unit_cost ? clock64() : 0;
     unsigned long long cnt = 0;
@@ -303,9 +363,9 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
         r = __shfl_sync(0xffffffffu, r, 0);
         klo = __shfl_sync(0xffffffffu, klo, 0);
         khi = __shfl_sync(0xffffffffu, khi, 0);
-        if (khi > klo) cnt += matrix_pairs(adj + r, klo, khi, lo, hwords, H, Sb, lane);
+        if (khi > klo) cnt += matrix_block_pairs<U>(adj + r, klo, khi, lo, hstride, H, Sb, lane);
     }
-    for (;;) {  // phase 2: 32 in-neighbours per grab
+    for (;;) {  // phase 2: 32 in-neighbours per grab, spans staged two deep
         unsigned long long q = 0;
         if (lane == 0) q = atomicAdd(&next[1], 32ull);
         const uint64_t base = __shfl_sync(0xffffffffu, q, 0) + c1;
@@ -315,15 +375,37 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
         uint32_t klo = 0, khi = 0;
         if (c < n) matrix_span(off, adj, dplus, lo, hi, c, &r, &klo, &khi);
         unsigned todo = __ballot_sync(0xffffffffu, khi > klo);
-        while (todo) {
-            const int src = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const int32_t* S = adj + __shfl_sync(0xffffffffu, r, src);
+        if (!todo) continue;
+        int src = __ffs(todo) - 1;
+        todo &= todo - 1;
+        int buf = 0;
+        int shift = stage_span(adj, __shfl_sync(0xffffffffu, r, src), __shfl_sync(0xffffffffu, khi, src),
+                               stage, lane);
+        cp_async_commit();
+        for (;;) {
+            const int nxt = todo ? __ffs(todo) - 1 : -1;
+            if (nxt >= 0) todo &= todo - 1;
+            int nshift = -1;
+            if (nxt >= 0)
+                nshift = stage_span(adj, __shfl_sync(0xffffffffu, r, nxt), __shfl_sync(0xffffffffu, khi, nxt),
+                                    stage + (buf ^ 1) * kStageVec, lane);
+            cp_async_commit();
+            cp_async_wait<1>();  // every group but the one just issued: the current span is in place
+            __syncwarp();
+            const uint64_t rs = __shfl_sync(0xffffffffu, r, src);
             const uint32_t j0 = __shfl_sync(0xffffffffu, klo, src);
             const uint32_t k = __shfl_sync(0xffffffffu, khi, src);
-            cnt += matrix_pairs(S, j0, k, lo, hwords, H, Sb, lane);
+            const int32_t* S = shift >= 0 ? reinterpret_cast<const int32_t*>(stage + buf * kStageVec) + shift
+                                          : adj + rs;
+            cnt += matrix_block_pairs<U>(S, j0, k, lo, hstride, H, Sb, lane);
+            __syncwarp();  // the buffer just read is the next stage's target
+            if (nxt < 0) break;
+            src = nxt;
+            shift = nshift;
+            buf ^= 1;
         }
     }
+    cp_async_wait<0>();
     if (unit_cost) {
         __syncwarp();
         if (lane == 0) atomicAdd(&unit_cost[unit], (unsigned long long)(clock64() - t0));
@@ -519,9 +601,36 @@ struct LaunchGroup {
     std::vector<int32_t> unit_ids;  // matrix groups: one launch per unit (ranges not merged)
 };
 
+// Words per resident pivot bitmap row of a matrix unit with ids below hi:
+// ceil(hi / 32) rounded up to 16 bytes, so rows can be read as uint4.
+static uint32_t matrix_stride(int64_t hi) { return (uint32_t)((((hi + 31) / 32) + 3) & ~(int64_t)3); }
+
 // Bytes of the resident pivot bitmap rows of a matrix unit [lo, hi).
-static uint64_t matrix_bytes(int64_t lo, int64_t hi) {
-    return (uint64_t)(hi - lo) * (uint64_t)((hi + 31) / 32) * 4;
+static uint64_t matrix_bytes(int64_t lo, int64_t hi) { return (uint64_t)(hi - lo) * matrix_stride(hi) * 4; }
+
+// Pivots per block of the matrix kernel: 4, or 8 with PC_MATRIX_PIVOT_BLOCK=8
+// in the environment (read once; a tuning override for measurements).
+static int matrix_pivot_block() {
+    static const int u = [] {
+        const char* e = getenv("PC_MATRIX_PIVOT_BLOCK");
+        return (e && atoi(e) == 8) ? 8 : 4;
+    }();
+    return u;
+}
+
+template <int U>
+static pc_status launch_matrix(pc_pgraph* pg, int64_t lo, int64_t hi, uint32_t hstride, const uint32_t* H,
+                               unsigned long long* d_next, unsigned long long* d_total, unsigned long long* d_cost,
+                               int32_t unit, int sms, cudaStream_t s) {
+    const size_t smem = (size_t)kMatrixWarps * hstride * 4 + (size_t)kMatrixWarps * 2 * kStageVec * sizeof(uint4);
+    PC_CUDA(cudaFuncSetAttribute(k_tc_matrix<U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    PC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_matrix<U>, kMatrixWarps * 32, smem));
+    k_tc_matrix<U><<<(unsigned)(sms * std::max(1, per_sm)), kMatrixWarps * 32, smem, s>>>(
+        pg->off, pg->adj, pg->dplus.as<uint32_t>(), (int32_t)lo, (int32_t)hi, pg->g->n, hstride, H, d_next, d_total,
+        d_cost, unit);
+    PC_LAUNCHED();
+    return PC_OK;
 }
 
 // The in-neighbour-major form over one unit (ids [lo, hi)), all asynchronous:
@@ -531,20 +640,16 @@ static pc_status run_matrix_unit(pc_pgraph* pg, int64_t lo, int64_t hi, int32_t 
                                  uint64_t* launches) {
     cudaStream_t s = pg->g->stream;
     const int sms = sm_count(pg->g->device);
-    const uint32_t hwords = (uint32_t)((hi + 31) / 32);
+    const uint32_t hstride = matrix_stride(hi);
     PC_CUDA(cudaMemsetAsync(H, 0, matrix_bytes(lo, hi), s));
     PC_CUDA(cudaMemsetAsync(d_next, 0, 16, s));
-    k_matrix_rows<<<sms * 8, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), (int32_t)lo, (int32_t)hi, hwords,
+    k_matrix_rows<<<sms * 8, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), (int32_t)lo, (int32_t)hi, hstride,
                                           H);
     PC_LAUNCHED();
-    const size_t smem = (size_t)kMatrixWarps * hwords * 4;
-    PC_CUDA(cudaFuncSetAttribute(k_tc_matrix, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    PC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_matrix, kMatrixWarps * 32, smem));
-    k_tc_matrix<<<(unsigned)(sms * std::max(1, per_sm)), kMatrixWarps * 32, smem, s>>>(
-        pg->off, pg->adj, pg->dplus.as<uint32_t>(), (int32_t)lo, (int32_t)hi, pg->g->n, hwords, H, d_next, d_total,
-        d_cost, unit);
-    PC_LAUNCHED();
+    if (matrix_pivot_block() == 8)
+        PC_TRY(launch_matrix<8>(pg, lo, hi, hstride, H, d_next, d_total, d_cost, unit, sms, s));
+    else
+        PC_TRY(launch_matrix<4>(pg, lo, hi, hstride, H, d_next, d_total, d_cost, unit, sms, s));
     *launches += 2;
     return PC_OK;
 }

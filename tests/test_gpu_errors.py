@@ -63,6 +63,8 @@ def test_rejects_bad_arguments(gpu):
     _raises_invalid(lambda: pg.solve_bfs(6))
     _raises_invalid(lambda: pg.solve_bfs(-1))
     _raises_invalid(lambda: pg.solve_sssp(7))
+    _raises_invalid(lambda: pg.solve_sssp(0, method=3))
+    _raises_invalid(lambda: pg.solve_sssp(0, method=pc.SSSP_DELTA_STEPPING, delta=-1))
     _raises_invalid(lambda: pg.batch_cnt_common_neis_merge(np.array([[0, 9]], np.int32)))
     _raises_invalid(lambda: pg.jaccard_queries(np.array([0, 6], np.int32)))
     _raises_invalid(lambda: pg.page_rank(0.85, 0))

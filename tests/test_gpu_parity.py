@@ -187,7 +187,13 @@ def test_frontier_algorithms(gpu, O, cases):
         pg = _pg(pc, g, v2p)
         for src in {0, n // 2, n - 1}:
             np.testing.assert_array_equal(pg.solve_bfs(src), O.bfs(vl, el, src), err_msg=f"{cid} bfs {src}")
-            np.testing.assert_array_equal(pg.solve_sssp(src), O.sssp(vl, el, w, src), err_msg=f"{cid} sssp {src}")
+            want = O.sssp(vl, el, w, src)
+            np.testing.assert_array_equal(pg.solve_sssp(src), want, err_msg=f"{cid} sssp {src}")
+            # every schedule and bucket width ends at the same exact distances
+            for method, delta in ((pc.SSSP_BELLMAN_FORD, 0), (pc.SSSP_DELTA_STEPPING, 0), (pc.SSSP_DELTA_STEPPING, 1),
+                                  (pc.SSSP_DELTA_STEPPING, 37), (pc.SSSP_DELTA_STEPPING, 1 << 29)):
+                np.testing.assert_array_equal(pg.solve_sssp(src, method=method, delta=delta), want,
+                                              err_msg=f"{cid} sssp {src} method {method} delta {delta}")
         ref64 = O.pagerank_f64(vl, el, 0.85, 20)
         np.testing.assert_allclose(pg.page_rank(0.85, 20, fp64=True), ref64, rtol=PR_F64_RTOL, atol=0, err_msg=cid)
         np.testing.assert_allclose(pg.page_rank(0.85, 20).astype(np.float64), ref64, rtol=PR_F32_RTOL, atol=0,
