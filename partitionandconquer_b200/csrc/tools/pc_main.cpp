@@ -69,6 +69,33 @@ string pfile(const string& dir, const string& method, int P) {
     return dir + "/partition/" + method + "/P" + to_string(P) + ".bin";
 }
 
+// The value the reference's serial k-core prints as "largest core"
+// (Graph::solve_kcore, src/Graph.cpp:681-718): k - 1 at the first level k
+// that finds no vertex left.  That is max core + 1 -- except when every
+// vertex of the max core C has exactly max-core neighbours in C, so the whole
+// of C goes in the first pass of its level and the next level never starts
+// (then max core) -- and 0 when the peeling never finishes (a complete
+// graph: the loop stops at k = n - 1 and every core reads 0, so a vertex of
+// positive degree has core 0).  The core numbers themselves are exact.
+int reference_largest_core_line(const Graph& g, const vector<int>& core) {
+    const int n = g.get_vertex_num();
+    if (n == 0) return 0;
+    const EID* vl = g.get_csr_vlist();
+    const VID* el = g.get_csr_elist();
+    int mx = 0;
+    for (int u = 0; u < n; ++u) {
+        if (core[u] == 0 && vl[u + 1] > vl[u]) return 0;
+        mx = max(mx, core[u]);
+    }
+    for (int u = 0; u < n; ++u) {
+        if (core[u] != mx) continue;
+        int inside = 0;
+        for (EID j = vl[u]; j < vl[u + 1]; ++j) inside += core[el[j]] == mx;
+        if (inside != mx) return mx + 1;
+    }
+    return mx;
+}
+
 void head(const char* what, const vector<int>& v) {
     for (size_t i = 0; i < min<size_t>(10, v.size()); ++i) printf("  vertex: %zu, %s: %d\n", i, what, v[i]);
     printf("  ... \n");
@@ -144,7 +171,7 @@ int run(int argc, char** argv) {
             t.start();
             G.solve_kcore(res);
             t.stop();
-            printf("largest core: %d.\n", res.empty() ? 0 : *max_element(res.begin(), res.end()));
+            printf("largest core: %d.\n", reference_largest_core_line(g, res));
             t.print(part ? "partitioned Core Decomposition" : "parallel Core Decomposition");
         } else if (task == "mis") {
             t.start();

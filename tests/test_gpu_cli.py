@@ -84,13 +84,29 @@ def test_cli_mis_and_cdlp(graph_dir, part):
     assert _ints(_run(PC_MAIN, args), pat) == _ints(_run(REF_MAIN, args), pat) != []
 
 
-def test_cli_kcore_largest_core(graph_dir):
-    d = graph_dir[0]
+def test_cli_kcore_largest_core(graph_dir, tmp_path):
+    """The line the reference's serial k-core prints is max core + 1, max core
+    when the max core is regular, and 0 for a complete graph; pc_main prints
+    the same line in both modes (the reference's partitioned task prints 0)."""
+    from conftest import csr_from_edges
     pat = r"largest core: (\d+)\."
-    want = _ints(_run(REF_MAIN, ["kcore", d, 0, "equal", 8, 4]), pat)
-    assert want and want[0] > 0
-    for part in (0, 1):
-        assert _ints(_run(PC_MAIN, ["kcore", d, part, "equal", 8, 4]), pat) == want
+    dirs = [graph_dir[0]]
+    for name, n, edges in (("k6", 6, [(i, j) for i in range(6) for j in range(i + 1, 6)]),
+                           ("k5tail", 7, [(i, j) for i in range(5) for j in range(i + 1, 5)] + [(4, 5), (5, 6)]),
+                           ("cycle", 6, [(0, 1), (1, 2), (2, 3), (3, 0)])):
+        d = tmp_path / name
+        (d / "origin").mkdir(parents=True)
+        (d / "partition" / "equal").mkdir(parents=True)
+        vl, el = csr_from_edges(n, edges)
+        vl.astype(np.uint64).tofile(d / "origin" / "csr_vlist.bin")
+        el.astype(np.int32).tofile(d / "origin" / "csr_elist.bin")
+        np.zeros(n, np.int32).tofile(d / "partition" / "equal" / "P8.bin")
+        dirs.append(d)
+    for d in dirs:
+        want = _ints(_run(REF_MAIN, ["kcore", d, 0, "equal", 8, 4]), pat)
+        assert want
+        for part in (0, 1):
+            assert _ints(_run(PC_MAIN, ["kcore", d, part, "equal", 8, 4]), pat) == want, d
 
 
 def test_cli_sssp(graph_dir):
