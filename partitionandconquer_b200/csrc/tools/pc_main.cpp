@@ -80,8 +80,8 @@ string pfile(const string& dir, const string& method, int P) {
 int reference_largest_core_line(const Graph& g, const vector<int>& core) {
     const int n = g.get_vertex_num();
     if (n == 0) return 0;
-    const EID* vl = g.get_csr_vlist();
-    const VID* el = g.get_csr_elist();
+    const pc::EID* vl = g.get_csr_vlist();
+    const pc::VID* el = g.get_csr_elist();
     int mx = 0;
     for (int u = 0; u < n; ++u) {
         if (core[u] == 0 && vl[u + 1] > vl[u]) return 0;
@@ -90,7 +90,7 @@ int reference_largest_core_line(const Graph& g, const vector<int>& core) {
     for (int u = 0; u < n; ++u) {
         if (core[u] != mx) continue;
         int inside = 0;
-        for (EID j = vl[u]; j < vl[u + 1]; ++j) inside += core[el[j]] == mx;
+        for (pc::EID j = vl[u]; j < vl[u + 1]; ++j) inside += core[el[j]] == mx;
         if (inside != mx) return mx + 1;
     }
     return mx;
