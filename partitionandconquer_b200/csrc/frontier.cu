@@ -351,6 +351,24 @@ __global__ void k_clear_flags(const int32_t* __restrict__ q, uint32_t qn, int32_
     if (i < qn) flag[q[i]] = 0;
 }
 
+// Hands the ids of adj[b, e) taken by lane gl of a group of L lanes to
+// f(ok, id), four per 16-byte load: the loads start at the 16-byte boundary
+// at or below b and step by 4 L ids, so one dependent round gives each lane
+// four independent gathers; ok is false for the positions of a load outside
+// [b, e), which the caller skips.  A load may run up to 3 ids past e, which
+// the 64 ids of padding after the last row keep inside the adjacency array.
+template <int L, class F>
+__device__ __forceinline__ void row_ids_vec4(const int32_t* __restrict__ adj, uint64_t b, uint64_t e, int gl,
+                                             F&& f) {
+    for (uint64_t q = (b & ~3ull) + 4ull * (uint64_t)gl; q < e; q += 4ull * L) {
+        const int4 v = __ldg(reinterpret_cast<const int4*>(adj + q));
+        f(q >= b, v.x);
+        f(q + 1 >= b && q + 1 < e, v.y);
+        f(q + 2 >= b && q + 2 < e, v.z);
+        f(q + 3 < e, v.w);
+    }
+}
+
 // ---- PageRank (pull) -----------------------------------------------------------
 
 template <class T>
@@ -399,7 +417,9 @@ __global__ void __launch_bounds__(kThreads) k_pr_iter(const uint64_t* __restrict
         const int32_t v = hq[h];
         const uint64_t b = off[v], e = off[v + 1];
         double s = 0.0;
-        for (uint64_t j = b + threadIdx.x; j < e; j += kThreads) s += (double)__ldg(contrib + adj[j]);
+        row_ids_vec4<kThreads>(adj, b, e, threadIdx.x, [&](bool ok, int32_t u) {
+            if (ok) s += (double)__ldg(contrib + u);
+        });
         for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0) s_part[wib] = s;
         __syncthreads();
@@ -424,7 +444,9 @@ __global__ void __launch_bounds__(kThreads) k_pr_iter(const uint64_t* __restrict
             if (e - b > kPullHeavyDeg) e = b;  // a CTA row
         }
         double s = 0.0;
-        for (uint64_t j = b + gl; j < e; j += kPullLanes) s += (double)__ldg(contrib + adj[j]);
+        row_ids_vec4<kPullLanes>(adj, b, e, gl, [&](bool ok, int32_t u) {
+            if (ok) s += (double)__ldg(contrib + u);
+        });
         for (int o = kPullLanes / 2; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (v < n && gl == 0 && off[v + 1] - off[v] <= kPullHeavyDeg) pr_epilogue(v, base, s, degs, x_out, contrib_out);
     }
@@ -814,7 +836,9 @@ __global__ void __launch_bounds__(kThreads) k_cdlp_iter(const uint64_t* __restri
         const int32_t v = hq[h];
         const uint64_t b = off[v], e = off[v + 1];
         int32_t mx = 0;
-        for (uint64_t j = b + threadIdx.x; j < e; j += kThreads) mx = max(mx, __ldg(lab + adj[j]));
+        row_ids_vec4<kThreads>(adj, b, e, threadIdx.x, [&](bool ok, int32_t u) {
+            if (ok) mx = max(mx, __ldg(lab + u));
+        });
         for (int o = 16; o; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
         if (lane == 0) s_part[wib] = mx;
         __syncthreads();
@@ -838,7 +862,9 @@ __global__ void __launch_bounds__(kThreads) k_cdlp_iter(const uint64_t* __restri
             if (e - b > kPullHeavyDeg) e = b;  // a CTA row
         }
         int32_t mx = 0;
-        for (uint64_t j = b + gl; j < e; j += kPullLanes) mx = max(mx, __ldg(lab + adj[j]));
+        row_ids_vec4<kPullLanes>(adj, b, e, gl, [&](bool ok, int32_t u) {
+            if (ok) mx = max(mx, __ldg(lab + u));
+        });
         for (int o = kPullLanes / 2; o; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
         if (v < n && gl == 0 && off[v + 1] - off[v] <= kPullHeavyDeg) out[v] = mx;
     }
