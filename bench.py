@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sample-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-config5", action="store_true",
+                    help="skip the learned-vs-plain measurement on config 5's RMAT-25 graph")
     ap.add_argument("--train-scale", type=int, default=22)
     ap.add_argument("--batch", action="store_true",
                     help="many-graph workload: 4096 RMAT graphs (scale 10..16, ef 8..32, seeds 0..4095), "
@@ -373,18 +375,22 @@ def run_reference_arm(args, dist):
 # ---- our arm ------------------------------------------------------------------------
 
 def train_selector(pc, args):
-    """Training data generated by the method itself on separate graphs (RMAT
-    at three scales with other seeds than the measured graph, ER and
-    Chung-Lu): in-situ per-unit costs
-    of every variant, one collection group per graph; the heuristic is
-    autotuned on the samples, then the MLP is trained on the GPU with its
-    judge margin chosen by leave-one-graph-out validation."""
+    """Training data generated by the method itself on separate graphs:
+    in-situ per-unit costs of every variant, one collection group per graph.
+    The graphs are RMAT at scales 20, 22 and 24 and two RMAT-25 graphs (all
+    with other seeds than the measured graphs), ER and Chung-Lu; each is
+    partitioned into 16 K-vertex units like the measured graphs.  The
+    heuristic is autotuned on the samples, then the MLP is trained on the GPU
+    (each unit weighted by its time) with its judge margin chosen by
+    leave-one-graph-out validation."""
     sel = pc.selector
     sel.clear()
     s = args.train_scale
     graphs = [lambda: pc.Graph.rmat_device(s - 2, args.edge_factor, args.seed + 4),
               lambda: pc.Graph.rmat_device(s, args.edge_factor, args.seed + 1),
               lambda: pc.Graph.rmat_device(s + 2, args.edge_factor, args.seed + 5),
+              lambda: pc.Graph.rmat_device(25, args.edge_factor, args.seed + 1),
+              lambda: pc.Graph.rmat_device(25, args.edge_factor, args.seed + 2),
               lambda: pc.Graph.er_device(s - 2, 1 << (s + 2), args.seed + 2),
               lambda: pc.Graph(host=pc.HostCSR.chung_lu(s - 2, 1 << (s + 2), 2.1, 1 << (s - 6), args.seed + 3))]
     for make in graphs:
@@ -400,7 +406,30 @@ def train_selector(pc, args):
     return {"samples": sel.num_samples(), "train_loss": loss, "heuristic_params": tuned.tolist(),
             "judge_margin": None if not np.isfinite(margin) else round(float(np.exp(margin)), 4),
             "heldout_gain_vs_plain": round(gain, 4),
+            "training_graphs": f"RMAT-{s - 2}/{s}/{s + 2} and RMAT-25 x2 (seeds {args.seed + 4}, {args.seed + 1}, "
+                               f"{args.seed + 5}, {args.seed + 1}, {args.seed + 2}), ER and Chung-Lu at 2^{s - 2}",
             "collection": "in-situ: every variant run on all units at once, each unit charged its cycle share"}
+
+
+def learned_vs_plain_config5(pc, torch, args):
+    """Config 5's graph (RMAT-25 ef16 seed 1, 2048 partitions) under the
+    trained selector: learned and plain plans timed back to back, both counts
+    checked against the pinned count (CSR fingerprint and T)."""
+    g = pc.Graph.rmat_device(25, args.edge_factor, args.seed)
+    vl, el = g.get_csr_vlist(), g.get_csr_elist()
+    name, t_pin = pinned_count(vl, el)
+    del vl, el
+    pg = pc.Partitioned_Graph(g, pc.equal_vertex_partition(g.get_vertex_num(), 2048))
+    stream = torch.cuda.ExternalStream(g.stream())
+    lp = _learned_vs_plain(pc, torch, pg, stream, max(3, args.steps // 2), 2)
+    lp["unit_cost_sums"] = plan_bounds(pc, pg)
+    lp["pinned"], lp["pinned_T"] = name, t_pin
+    lp["match"] = t_pin is not None and lp["triangles"] == t_pin
+    pg.close()
+    g.close()
+    if not lp["match"]:
+        raise SystemExit(f"RMAT-25 count differs from the pinned value: {lp}")
+    return {"workload": "tc_rmat25_ef16_p2048", **lp}
 
 
 def plan_bounds(pc, pg):
@@ -540,6 +569,7 @@ def run_ours(args, dist):
     for a in pinned:
         L.lib.pc_host_unregister(L.ptr(a))
     bounds = plan_bounds(pc, pg)
+    cfg5 = learned_vs_plain_config5(pc, torch, args) if not args.no_config5 else None
     e2e_s = dist.max(statistics.median(e2e))
     e2e_value = dist.world * e_plus / e2e_s / 1e9
     h2d = vl.nbytes + el.nbytes + v2p.nbytes
@@ -572,6 +602,7 @@ def run_ours(args, dist):
                                  "speedup": round(plain_ms / step_ms, 4),
                                  "plain_variants_per_unit": list(st_plain.variant_hist),
                                  "unit_cost_sums": bounds, **train},
+            "learned_vs_plain_config5": cfg5,
             "e2e": {"value": round(e2e_value, 4), "unit": "GTEPS", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": 8, "ms_per_step": round(e2e_s * 1e3, 2),
                     "phases_ms": dict(zip(("upload_validate", "partition_view", "features_plan_count", "release"),

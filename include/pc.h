@@ -382,6 +382,11 @@ int32_t pc_mlp_num_params(void);
 pc_status pc_mlp_forward(const float* params, const float* x, int32_t batch, float* y);
 pc_status pc_mlp_loss_grad(const float* params, const float* x, const float* y, const uint8_t* mask, int32_t batch,
                            float* loss, float* grad);
+/* The same with each sample's squared errors weighted by weights[batch]
+ * (NULL: all 1): the loss the selector's training minimises, with every
+ * unit weighted by the measured time of its fastest variant. */
+pc_status pc_mlp_loss_grad_weighted(const float* params, const float* x, const float* y, const uint8_t* mask,
+                                    const float* weights, int32_t batch, float* loss, float* grad);
 pc_status pc_mlp_train_steps(float* params, const float* x, const float* y, const uint8_t* mask, int32_t batch,
                              int32_t steps, float lr, float* final_loss);
 

@@ -151,6 +151,7 @@ _SIG = {
     "pc_mlp_num_params": (i32, []),
     "pc_mlp_forward": (i32, [P, P, i32, P]),
     "pc_mlp_loss_grad": (i32, [P, P, P, P, i32, P, P]),
+    "pc_mlp_loss_grad_weighted": (i32, [P, P, P, P, P, i32, P, P]),
     "pc_mlp_train_steps": (i32, [P, P, P, P, i32, i32, f32, P]),
     "pc_synth_rmat": (i32, [u32, u32, u64, i32, PP]),
     "pc_synth_er": (i32, [u32, u64, u64, i32, PP]),

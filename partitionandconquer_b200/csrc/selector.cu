@@ -99,6 +99,7 @@ struct TrainSmem {
     float x[kChunkS][kMlpIn];
     float t[kChunkS][kMlpOut];
     float msk[kChunkS][kMlpOut];
+    float w[kChunkS];
     float h1[kChunkS][kMlpHidden];
     float h2[kChunkS][kMlpHidden];
     float y[kChunkS][kMlpOut];
@@ -110,12 +111,14 @@ struct TrainSmem {
 };
 
 // Full-batch training: `steps` iterations of forward, backward (mean squared
-// error over masked outputs) and Adam.  With steps == 0 the kernel evaluates
-// the loss and gradient at `params` (gradient check) without updating.
+// error over masked outputs, each sample's terms weighted by W[s], 1 when W
+// is null) and Adam.  With steps == 0 the kernel evaluates the loss and
+// gradient at `params` (gradient check) without updating.
 __global__ void __launch_bounds__(kTrainThreads) k_mlp_train(float* __restrict__ params, float* __restrict__ adam_m,
                                                              float* __restrict__ adam_v, const float* __restrict__ X,
                                                              const float* __restrict__ Y,
-                                                             const uint8_t* __restrict__ M, int batch, float inv_count,
+                                                             const uint8_t* __restrict__ M,
+                                                             const float* __restrict__ W, int batch, float inv_count,
                                                              int steps, float lr, float* __restrict__ loss_out,
                                                              float* __restrict__ grad_out) {
     extern __shared__ float4 smem_raw[];
@@ -140,6 +143,7 @@ __global__ void __launch_bounds__(kTrainThreads) k_mlp_train(float* __restrict__
                 S.t[s][o] = s < ns ? Y[(size_t)(c0 + s) * kMlpOut + o] : 0.f;
                 S.msk[s][o] = (s < ns && M[(size_t)(c0 + s) * kMlpOut + o]) ? 1.f : 0.f;
             }
+            for (int s = tid; s < kChunkS; s += blockDim.x) S.w[s] = s < ns ? (W ? W[c0 + s] : 1.f) : 0.f;
             __syncthreads();
             for (int i = tid; i < kChunkS * kMlpHidden; i += blockDim.x) {
                 const int s = i / kMlpHidden, j = i % kMlpHidden;
@@ -161,8 +165,8 @@ __global__ void __launch_bounds__(kTrainThreads) k_mlp_train(float* __restrict__
                 for (int k = 0; k < kMlpHidden; ++k) z += S.P[kOffW3 + o * kMlpHidden + k] * S.h2[s][k];
                 S.y[s][o] = z;
                 const float d = (z - S.t[s][o]) * S.msk[s][o];
-                S.dy[s][o] = 2.f * d * inv_count;
-                S.lpart[i] = d * d * inv_count;
+                S.dy[s][o] = 2.f * S.w[s] * d * inv_count;
+                S.lpart[i] = S.w[s] * d * d * inv_count;
             }
             __syncthreads();
             if (tid == 0) {
@@ -295,12 +299,12 @@ static size_t train_smem_bytes() { return sizeof(TrainSmem) + 16; }
 
 // Runs the training kernel on the current device.
 static pc_status run_train_kernel(std::vector<float>& params, const std::vector<float>& X, const std::vector<float>& Y,
-                                  const std::vector<uint8_t>& M, int batch, int steps, float lr, float* loss,
-                                  std::vector<float>* grad) {
+                                  const std::vector<uint8_t>& M, const std::vector<float>* W, int batch, int steps,
+                                  float lr, float* loss, std::vector<float>* grad) {
     size_t cnt = 0;
     for (int i = 0; i < batch * kMlpOut; ++i) cnt += M[i] ? 1 : 0;
     if (cnt == 0) return fail(PC_ERR_INVALID_INPUT, "no masked targets to train on");
-    DevBuf dP, dm, dv, dX, dY, dM, dL, dG;
+    DevBuf dP, dm, dv, dX, dY, dM, dW, dL, dG;
     PC_TRY(dP.alloc(kMlpParams * 4, "mlp params"));
     PC_TRY(dm.alloc(kMlpParams * 4, "adam m"));
     PC_TRY(dv.alloc(kMlpParams * 4, "adam v"));
@@ -315,10 +319,15 @@ static pc_status run_train_kernel(std::vector<float>& params, const std::vector<
     PC_CUDA(cudaMemcpy(dX.p, X.data(), (size_t)batch * kMlpIn * 4, cudaMemcpyHostToDevice));
     PC_CUDA(cudaMemcpy(dY.p, Y.data(), (size_t)batch * kMlpOut * 4, cudaMemcpyHostToDevice));
     PC_CUDA(cudaMemcpy(dM.p, M.data(), (size_t)batch * kMlpOut, cudaMemcpyHostToDevice));
+    if (W) {
+        PC_TRY(dW.alloc((size_t)batch * 4, "mlp sample weights"));
+        PC_CUDA(cudaMemcpy(dW.p, W->data(), (size_t)batch * 4, cudaMemcpyHostToDevice));
+    }
     const size_t smem = train_smem_bytes();
     PC_CUDA(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_mlp_train<<<1, kTrainThreads, smem>>>(dP.as<float>(), dm.as<float>(), dv.as<float>(), dX.as<float>(),
-                                            dY.as<float>(), dM.as<uint8_t>(), batch, 1.0f / (float)cnt, steps, lr,
+                                            dY.as<float>(), dM.as<uint8_t>(), W ? dW.as<float>() : nullptr, batch,
+                                            1.0f / (float)cnt, steps, lr,
                                             dL.as<float>(), dG.as<float>());
     PC_LAUNCHED();
     PC_CUDA(cudaDeviceSynchronize());
@@ -437,14 +446,21 @@ pc_status pc_mlp_forward(const float* params, const float* x, int32_t batch, flo
 
 pc_status pc_mlp_loss_grad(const float* params, const float* x, const float* y, const uint8_t* mask, int32_t batch,
                            float* loss, float* grad) {
+    return pc_mlp_loss_grad_weighted(params, x, y, mask, nullptr, batch, loss, grad);
+}
+
+pc_status pc_mlp_loss_grad_weighted(const float* params, const float* x, const float* y, const uint8_t* mask,
+                                    const float* weights, int32_t batch, float* loss, float* grad) {
     clear_error();
     if (!params || !x || !y || !mask || batch <= 0) return fail(PC_ERR_INVALID_INPUT, "bad argument");
     if (pc_device_count() == 0) return fail(PC_ERR_NO_DEVICE, "no CUDA device is visible");
     std::vector<float> p(params, params + kMlpParams);
     std::vector<float> X(x, x + (size_t)batch * kMlpIn), Y(y, y + (size_t)batch * kMlpOut);
     std::vector<uint8_t> M(mask, mask + (size_t)batch * kMlpOut);
+    std::vector<float> W;
+    if (weights) W.assign(weights, weights + batch);
     std::vector<float> g;
-    PC_TRY(run_train_kernel(p, X, Y, M, batch, 0, 0.f, loss, &g));
+    PC_TRY(run_train_kernel(p, X, Y, M, weights ? &W : nullptr, batch, 0, 0.f, loss, &g));
     if (grad) memcpy(grad, g.data(), kMlpParams * 4);
     return PC_OK;
 }
@@ -457,7 +473,7 @@ pc_status pc_mlp_train_steps(float* params, const float* x, const float* y, cons
     std::vector<float> p(params, params + kMlpParams);
     std::vector<float> X(x, x + (size_t)batch * kMlpIn), Y(y, y + (size_t)batch * kMlpOut);
     std::vector<uint8_t> M(mask, mask + (size_t)batch * kMlpOut);
-    PC_TRY(run_train_kernel(p, X, Y, M, batch, steps, lr, final_loss, nullptr));
+    PC_TRY(run_train_kernel(p, X, Y, M, nullptr, batch, steps, lr, final_loss, nullptr));
     memcpy(params, p.data(), kMlpParams * 4);
     return PC_OK;
 }
@@ -681,20 +697,36 @@ namespace pc {
 
 // Fits a model to the samples idx of `data` (standardisation, He-uniform
 // initialisation from the counter-based generator, full-batch Adam on the GPU).
+// Each sample's squared errors are weighted by the measured time of its
+// unit's fastest variant (normalised to mean 1 over the fit): the quantity
+// the selector minimises is the summed time, so the few units that hold most
+// of it -- the hub units, a handful among hundreds -- must be predicted
+// well, not just the many light ones.
 static pc_status fit_model(const Model& data, const std::vector<size_t>& idx, int32_t steps, float lr, uint64_t seed,
                            Model* md, float* loss) {
     const int n = (int)idx.size();
-    std::vector<float> X((size_t)n * kMlpIn), Y((size_t)n * kMlpOut);
+    std::vector<float> X((size_t)n * kMlpIn), Y((size_t)n * kMlpOut), W((size_t)n, 1.f);
     std::vector<uint8_t> M((size_t)n * kMlpOut);
+    double wsum = 0.0;
     for (int i = 0; i < n; ++i) {
         const float* f = &data.feats[idx[i] * kNumFeatures];
         features_to_inputs(f, &X[(size_t)i * kMlpIn]);
         const float lw = log_work(f);
+        float best = INFINITY;
         for (int o = 0; o < kMlpOut; ++o) {
-            Y[(size_t)i * kMlpOut + o] = data.logms[idx[i] * kMlpOut + o] - lw;
-            M[(size_t)i * kMlpOut + o] = data.mask[idx[i] * kMlpOut + o];
+            const float lm = data.logms[idx[i] * kMlpOut + o];
+            const uint8_t mk = data.mask[idx[i] * kMlpOut + o];
+            Y[(size_t)i * kMlpOut + o] = lm - lw;
+            M[(size_t)i * kMlpOut + o] = mk;
+            if (mk) best = std::min(best, lm);
         }
+        W[i] = std::isfinite(best) ? (float)std::exp((double)best) : 0.f;
+        wsum += W[i];
     }
+    if (wsum > 0.0)
+        for (int i = 0; i < n; ++i) W[i] = (float)(W[i] * n / wsum);
+    else
+        std::fill(W.begin(), W.end(), 1.f);
     for (int k = 0; k < kMlpIn; ++k) {
         double m = 0, v = 0;
         for (int i = 0; i < n; ++i) m += X[(size_t)i * kMlpIn + k];
@@ -724,7 +756,7 @@ static pc_status fit_model(const Model& data, const std::vector<size_t>& idx, in
     init(kOffW1, kMlpIn, kMlpHidden * kMlpIn);
     init(kOffW2, kMlpHidden, kMlpHidden * kMlpHidden);
     init(kOffW3, kMlpHidden, kMlpOut * kMlpHidden);
-    return run_train_kernel(md->params, X, Y, M, n, steps, lr, loss, nullptr);
+    return run_train_kernel(md->params, X, Y, M, &W, n, steps, lr, loss, nullptr);
 }
 
 // Predicted log(ms) per variant for the samples idx of `data` under model md.

@@ -160,6 +160,21 @@ def mlp_loss_grad(params, x, y, mask):
     return float(loss.value), grad
 
 
+def mlp_loss_grad_weighted(params, x, y, mask, weights):
+    p = _lib.as_array(params, np.float32)
+    xx = _lib.as_array(x, np.float32).reshape(-1, MLP_IN)
+    yy = _lib.as_array(y, np.float32).reshape(-1, MLP_OUT)
+    mm = _lib.as_array(mask, np.uint8).reshape(-1, MLP_OUT)
+    ww = _lib.as_array(weights, np.float32)
+    if ww.size != xx.shape[0]:
+        raise ValueError("one weight per sample")
+    loss = C.c_float()
+    grad = np.empty(p.size, np.float32)
+    check(lib.pc_mlp_loss_grad_weighted(ptr(p), ptr(xx), ptr(yy), ptr(mm), ptr(ww), xx.shape[0], C.byref(loss),
+                                        ptr(grad)))
+    return float(loss.value), grad
+
+
 def mlp_train_steps(params, x, y, mask, steps: int, lr: float):
     p = _lib.as_array(params, np.float32).copy()
     xx = _lib.as_array(x, np.float32).reshape(-1, MLP_IN)
