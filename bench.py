@@ -377,8 +377,9 @@ def run_reference_arm(args, dist):
 def train_selector(pc, args):
     """Training data generated by the method itself on separate graphs:
     in-situ per-unit costs of every variant, one collection group per graph.
-    The graphs are RMAT at scales 20, 22 and 24 and two RMAT-25 graphs (all
-    with other seeds than the measured graphs), ER and Chung-Lu; each is
+    The graphs are RMAT at scales 20, 22 and 24 and two RMAT-25 graphs, ER
+    at 2^20, and Chung-Lu at 2^20 (mean degree 8) and 2^22 (mean degree 32,
+    as config 3's), all with other seeds than the measured graphs; each is
     partitioned into 16 K-vertex units like the measured graphs.  The
     heuristic is autotuned on the samples, then the MLP is trained on the GPU
     (each unit weighted by its time) with its judge margin chosen by
@@ -392,7 +393,8 @@ def train_selector(pc, args):
               lambda: pc.Graph.rmat_device(25, args.edge_factor, args.seed + 1),
               lambda: pc.Graph.rmat_device(25, args.edge_factor, args.seed + 2),
               lambda: pc.Graph.er_device(s - 2, 1 << (s + 2), args.seed + 2),
-              lambda: pc.Graph(host=pc.HostCSR.chung_lu(s - 2, 1 << (s + 2), 2.1, 1 << (s - 6), args.seed + 3))]
+              lambda: pc.Graph(host=pc.HostCSR.chung_lu(s - 2, 1 << (s + 2), 2.1, 1 << (s - 6), args.seed + 3)),
+              lambda: pc.Graph(host=pc.HostCSR.chung_lu(s, 1 << (s + 4), 2.1, 1 << (s - 4), args.seed + 6))]
     for make in graphs:
         g = make()
         n = g.get_vertex_num()
@@ -407,7 +409,8 @@ def train_selector(pc, args):
             "judge_margin": None if not np.isfinite(margin) else round(float(np.exp(margin)), 4),
             "heldout_gain_vs_plain": round(gain, 4),
             "training_graphs": f"RMAT-{s - 2}/{s}/{s + 2} and RMAT-25 x2 (seeds {args.seed + 4}, {args.seed + 1}, "
-                               f"{args.seed + 5}, {args.seed + 1}, {args.seed + 2}), ER and Chung-Lu at 2^{s - 2}",
+                               f"{args.seed + 5}, {args.seed + 1}, {args.seed + 2}), ER at 2^{s - 2}, Chung-Lu at "
+                               f"2^{s - 2} (mean degree 8) and 2^{s} (mean degree 32)",
             "collection": "in-situ: every variant run on all units at once, each unit charged its cycle share"}
 
 

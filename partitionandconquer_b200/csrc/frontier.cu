@@ -357,11 +357,13 @@ __global__ void k_clear_flags(const int32_t* __restrict__ q, uint32_t qn, int32_
 // four independent gathers; ok is false for the positions of a load outside
 // [b, e), which the caller skips.  A load may run up to 3 ids past e, which
 // the 64 ids of padding after the last row keep inside the adjacency array.
+// The adjacency is read once per sweep, so its loads carry the streaming
+// hint (evict first): the gathered vectors keep their L2 lines.
 template <int L, class F>
 __device__ __forceinline__ void row_ids_vec4(const int32_t* __restrict__ adj, uint64_t b, uint64_t e, int gl,
                                              F&& f) {
     for (uint64_t q = (b & ~3ull) + 4ull * (uint64_t)gl; q < e; q += 4ull * L) {
-        const int4 v = __ldg(reinterpret_cast<const int4*>(adj + q));
+        const int4 v = __ldcs(reinterpret_cast<const int4*>(adj + q));
         f(q >= b, v.x);
         f(q + 1 >= b && q + 1 < e, v.y);
         f(q + 2 >= b && q + 2 < e, v.z);
