@@ -241,8 +241,8 @@ pc_status pc_sssp(pc_pgraph* pg, int32_t src, int32_t* dist);
  *                          vertex is relaxed in the next round;
  *   PC_SSSP_DELTA_STEPPING delta-stepping (near/far piles): only vertices whose
  *                          distance is below the current bucket bound are
- *                          relaxed; buckets are `delta` wide (0: 32 x mean
- *                          weight / mean degree, computed on the device);
+ *                          relaxed; buckets are `delta` wide (0: 8 x mean
+ *                          weight, computed on the device);
  *   PC_SSSP_AUTO           delta-stepping with delta chosen from the graph. */
 #define PC_SSSP_AUTO 0
 #define PC_SSSP_BELLMAN_FORD 1

@@ -1107,16 +1107,20 @@ pc_status pc_sssp_ex(pc_pgraph* pg, int32_t src, int32_t method, int32_t delta, 
     if (use_delta) {
         PC_CUDA(cudaMemsetAsync(farflag, 0, n * 4, s));
         if (delta == 0) {
-            // Delta ~ 32 x mean weight / mean degree: about a warp's worth of
-            // improvements per vertex and bucket (Davidson et al.)
+            // Delta = 8 x mean weight.  Each relaxation round costs a launch and
+            // a host read of the queue size, so narrow buckets (many rounds per
+            // bucket) lose: on RMAT-22/24 with weights 1..255 the width of
+            // 32 x mean weight / mean degree (134; Davidson et al.) ran 1.3x
+            // slower than Bellman-Ford, while widths of 1024 and above ran 1-2 %
+            // faster than it.
             PC_CUDA(cudaMemsetAsync(wsum, 0, 8, s));
             k_sum_i32<<<grid_for(pg), kThreads, 0, s>>>(pg->w, m, wsum);
             PC_LAUNCHED();
             unsigned long long h = 0;
             PC_CUDA(cudaMemcpyAsync(&h, wsum, 8, cudaMemcpyDeviceToHost, s));
             PC_TRY(sync(pg));
-            const double mean_w = m ? (double)h / (double)m : 1.0, mean_d = n ? (double)m / (double)n : 1.0;
-            delta = (int32_t)std::min<double>(1 << 30, std::max(1.0, std::round(32.0 * mean_w / std::max(1.0, mean_d))));
+            const double mean_w = m ? (double)h / (double)m : 1.0;
+            delta = (int32_t)std::min<double>(1 << 30, std::max(1.0, std::round(8.0 * mean_w)));
         }
         bucket = delta;
     }

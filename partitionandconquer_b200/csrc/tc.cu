@@ -253,17 +253,11 @@ __device__ __forceinline__ bool matrix_words_win(int32_t b, uint32_t jl) {
 //    b, so words past a pivot's own length read zeros.
 // The form is chosen per block by the rounds each needs; the bitmap is built
 // only when some block uses it.  S may point to shared or global memory.
-// kVC (per-vertex counts, LCC): every pair (b, c) adds its hits to t(b)
-// (one warp reduction and atomic per pivot), the in-neighbour's hits go to
-// t(c) once per call (by the caller), and every hit a adds 1 to t(a) through
-// count_vertex (a per-CTA shared histogram for the hub ids).
-template <int U, bool kVC = false>
+template <int U>
 __device__ __forceinline__ unsigned long long matrix_block_pairs(const int32_t* S, uint32_t j0, uint32_t k,
                                                                  int32_t lo, uint32_t hstride,
                                                                  const uint32_t* __restrict__ H, uint32_t* Sb,
-                                                                 int lane,
-                                                                 unsigned long long* __restrict__ tri = nullptr,
-                                                                 uint32_t* hist = nullptr) {
+                                                                 int lane) {
     unsigned long long cnt = 0;
     bool want = false;
     for (uint32_t jb = j0 + (uint32_t)lane * U; jb < k; jb += 32u * U) {
@@ -283,12 +277,10 @@ __device__ __forceinline__ unsigned long long matrix_block_pairs(const int32_t* 
         const uint32_t ju = min((uint32_t)U, k - jb), jl = jb + ju - 1;
         const int32_t bl = S[jl];
         const uint32_t* h[U];
-        uint32_t hb[U];  // kVC: this lane's hits per pivot of the block
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const int32_t b = (uint32_t)u < ju ? S[jb + u] : bl;
             h[u] = H + (uint64_t)(b - lo) * hstride;
-            hb[u] = 0;
         }
         if (words && matrix_words_win(bl, jl)) {
             const uint32_t nv = ((((uint32_t)bl + 31) >> 5) + 3) >> 2;
@@ -298,22 +290,7 @@ __device__ __forceinline__ unsigned long long matrix_block_pairs(const int32_t* 
                 for (int u = 0; u < U; ++u) {
                     if ((uint32_t)u < ju) {
                         const uint4 v = __ldg(reinterpret_cast<const uint4*>(h[u]) + x);
-                        if constexpr (kVC) {
-                            const uint32_t wv[4] = {v.x & sv.x, v.y & sv.y, v.z & sv.z, v.w & sv.w};
-#pragma unroll
-                            for (int t = 0; t < 4; ++t) {
-                                uint32_t bits = wv[t];
-                                hb[u] += __popc(bits);
-                                while (bits) {
-                                    const int32_t a = (int32_t)((4 * x + t) * 32 + (uint32_t)(__ffs(bits) - 1));
-                                    bits &= bits - 1;
-                                    count_vertex(a, tri, hist);
-                                }
-                            }
-                        } else {
-                            cnt += __popc(v.x & sv.x) + __popc(v.y & sv.y) + __popc(v.z & sv.z) +
-                                   __popc(v.w & sv.w);
-                        }
+                        cnt += __popc(v.x & sv.x) + __popc(v.y & sv.y) + __popc(v.z & sv.z) + __popc(v.w & sv.w);
                     }
                 }
             }
@@ -322,25 +299,8 @@ __device__ __forceinline__ unsigned long long matrix_block_pairs(const int32_t* 
                 const int32_t a = S[i];
                 const uint32_t w = (uint32_t)a >> 5, bit = (uint32_t)a & 31;
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    if ((uint32_t)u < ju && i < jb + (uint32_t)u) {
-                        const uint32_t hit = (__ldg(h[u] + w) >> bit) & 1u;
-                        if constexpr (kVC) {
-                            hb[u] += hit;
-                            if (hit) count_vertex(a, tri, hist);
-                        } else {
-                            cnt += hit;
-                        }
-                    }
-                }
-            }
-        }
-        if constexpr (kVC) {
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t t = __reduce_add_sync(0xffffffffu, hb[u]);
-                cnt += hb[u];
-                if (lane == 0 && t && (uint32_t)u < ju) atomicAdd(&tri[S[jb + u]], (unsigned long long)t);
+                for (int u = 0; u < U; ++u)
+                    if ((uint32_t)u < ju && i < jb + (uint32_t)u) cnt += (__ldg(h[u] + w) >> bit) & 1u;
             }
         }
     }
@@ -373,7 +333,7 @@ __device__ __forceinline__ void matrix_span(const uint64_t* __restrict__ off, co
 // hubs at the end of the launch.
 constexpr uint64_t kMatrixHeavy = 65536;
 
-template <int U, bool kVC = false>
+template <int U>
 __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t* __restrict__ off,
                                                                const int32_t* __restrict__ adj,
                                                                const uint32_t* __restrict__ dplus, int32_t lo,
@@ -382,26 +342,12 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
                                                                unsigned long long* __restrict__ next,
                                                                unsigned long long* __restrict__ total,
                                                                unsigned long long* __restrict__ unit_cost,
-                                                               int32_t unit,
-                                                               unsigned long long* __restrict__ tri = nullptr) {
+                                                               int32_t unit) {
     extern __shared__ uint4 msm4[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     uint32_t* Sb = reinterpret_cast<uint32_t*>(msm4) + (size_t)w * hstride;  // warp-private bitmap of S_c
     uint4* stage = msm4 + (size_t)kMatrixWarps * (hstride / 4) + (size_t)w * 2 * kStageVec;
-    // kVC: per-CTA counts of the hub ids, after the stages
-    uint32_t* hist = reinterpret_cast<uint32_t*>(msm4 + (size_t)kMatrixWarps * (hstride / 4 + 2 * kStageVec));
     for (uint32_t i = lane; i < hstride; i += 32) Sb[i] = 0;
-    if constexpr (kVC) {
-        for (uint32_t i = threadIdx.x; i < (uint32_t)kHubHist; i += blockDim.x) hist[i] = 0;
-        __syncthreads();
-    }
-    // kVC: the in-neighbour's hits, all pivots of the call, go to t(c)
-    auto add_c = [&](uint64_t c, unsigned long long cc) {
-        if constexpr (kVC) {
-            const uint32_t t = __reduce_add_sync(0xffffffffu, (uint32_t)cc);
-            if (lane == 0 && t) atomicAdd(&tri[c], (unsigned long long)t);
-        }
-    };
     __syncwarp();
     const long long t0 = unit_cost ? clock64() : 0;
     unsigned long long cnt = 0;
@@ -417,12 +363,7 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
         r = __shfl_sync(0xffffffffu, r, 0);
         klo = __shfl_sync(0xffffffffu, klo, 0);
         khi = __shfl_sync(0xffffffffu, khi, 0);
-        if (khi > klo) {
-            const unsigned long long cc = matrix_block_pairs<U, kVC>(adj + r, klo, khi, lo, hstride, H, Sb, lane,
-                                                                     tri, hist);
-            cnt += cc;
-            add_c(c, cc);
-        }
+        if (khi > klo) cnt += matrix_block_pairs<U>(adj + r, klo, khi, lo, hstride, H, Sb, lane);
     }
     for (;;) {  // phase 2: 32 in-neighbours per grab, spans staged two deep
         unsigned long long q = 0;
@@ -456,9 +397,7 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
             const uint32_t k = __shfl_sync(0xffffffffu, khi, src);
             const int32_t* S = shift >= 0 ? reinterpret_cast<const int32_t*>(stage + buf * kStageVec) + shift
                                           : adj + rs;
-            const unsigned long long cc = matrix_block_pairs<U, kVC>(S, j0, k, lo, hstride, H, Sb, lane, tri, hist);
-            cnt += cc;
-            add_c(base + (uint64_t)src, cc);
+            cnt += matrix_block_pairs<U>(S, j0, k, lo, hstride, H, Sb, lane);
             __syncwarp();  // the buffer just read is the next stage's target
             if (nxt < 0) break;
             src = nxt;
@@ -473,11 +412,6 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
     }
     for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if (lane == 0 && cnt) atomicAdd(total, cnt);
-    if constexpr (kVC) {
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < (uint32_t)kHubHist; i += blockDim.x)
-            if (hist[i]) atomicAdd(&tri[i], (unsigned long long)hist[i]);
-    }
 }
 
 constexpr uint32_t kBitmapCapBits = 1u << 20;  // 128 KB of shared memory
@@ -684,18 +618,17 @@ static int matrix_pivot_block() {
     return u;
 }
 
-template <int U, bool kVC>
+template <int U>
 static pc_status launch_matrix(pc_pgraph* pg, int64_t lo, int64_t hi, uint32_t hstride, const uint32_t* H,
                                unsigned long long* d_next, unsigned long long* d_total, unsigned long long* d_cost,
-                               int32_t unit, int sms, cudaStream_t s, unsigned long long* d_tri) {
-    const size_t smem = (size_t)kMatrixWarps * hstride * 4 + (size_t)kMatrixWarps * 2 * kStageVec * sizeof(uint4) +
-                        (kVC ? (size_t)kHubHist * 4 : 0);
-    PC_CUDA(cudaFuncSetAttribute(k_tc_matrix<U, kVC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                               int32_t unit, int sms, cudaStream_t s) {
+    const size_t smem = (size_t)kMatrixWarps * hstride * 4 + (size_t)kMatrixWarps * 2 * kStageVec * sizeof(uint4);
+    PC_CUDA(cudaFuncSetAttribute(k_tc_matrix<U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    PC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_matrix<U, kVC>, kMatrixWarps * 32, smem));
-    k_tc_matrix<U, kVC><<<(unsigned)(sms * std::max(1, per_sm)), kMatrixWarps * 32, smem, s>>>(
+    PC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_matrix<U>, kMatrixWarps * 32, smem));
+    k_tc_matrix<U><<<(unsigned)(sms * std::max(1, per_sm)), kMatrixWarps * 32, smem, s>>>(
         pg->off, pg->adj, pg->dplus.as<uint32_t>(), (int32_t)lo, (int32_t)hi, pg->g->n, hstride, H, d_next, d_total,
-        d_cost, unit, d_tri);
+        d_cost, unit);
     PC_LAUNCHED();
     return PC_OK;
 }
@@ -704,7 +637,7 @@ static pc_status launch_matrix(pc_pgraph* pg, int64_t lo, int64_t hi, uint32_t h
 // rows H built from N+(b), then the walk over the in-neighbours.
 static pc_status run_matrix_unit(pc_pgraph* pg, int64_t lo, int64_t hi, int32_t unit, uint32_t* H,
                                  unsigned long long* d_next, unsigned long long* d_total, unsigned long long* d_cost,
-                                 uint64_t* launches, unsigned long long* d_tri) {
+                                 uint64_t* launches) {
     cudaStream_t s = pg->g->stream;
     const int sms = sm_count(pg->g->device);
     const uint32_t hstride = matrix_stride(hi);
@@ -713,12 +646,10 @@ static pc_status run_matrix_unit(pc_pgraph* pg, int64_t lo, int64_t hi, int32_t 
     k_matrix_rows<<<sms * 8, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), (int32_t)lo, (int32_t)hi, hstride,
                                           H);
     PC_LAUNCHED();
-    if (d_tri)
-        PC_TRY((launch_matrix<4, true>(pg, lo, hi, hstride, H, d_next, d_total, d_cost, unit, sms, s, d_tri)));
-    else if (matrix_pivot_block() == 8)
-        PC_TRY((launch_matrix<8, false>(pg, lo, hi, hstride, H, d_next, d_total, d_cost, unit, sms, s, nullptr)));
+    if (matrix_pivot_block() == 8)
+        PC_TRY(launch_matrix<8>(pg, lo, hi, hstride, H, d_next, d_total, d_cost, unit, sms, s));
     else
-        PC_TRY((launch_matrix<4, false>(pg, lo, hi, hstride, H, d_next, d_total, d_cost, unit, sms, s, nullptr)));
+        PC_TRY(launch_matrix<4>(pg, lo, hi, hstride, H, d_next, d_total, d_cost, unit, sms, s));
     *launches += 2;
     return PC_OK;
 }
@@ -741,7 +672,7 @@ static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long l
         if (!H || !d_next) return fail(PC_ERR_OOM, "scratch arena too small (internal sizing error)");
         for (size_t i = 0; i < gr.unit_ids.size(); ++i)
             PC_TRY(run_matrix_unit(pg, gr.ranges[2 * i], gr.ranges[2 * i + 1], gr.unit_ids[i], H, d_next, d_total,
-                                   d_cost, launches, d_tri));
+                                   d_cost, launches));
         return PC_OK;
     }
     const int32_t* unit_of = pg->unit_of.as<int32_t>();
@@ -1049,8 +980,8 @@ pc_status tc_count(pc_pgraph* pg, int32_t variant, uint64_t* count, pc_tc_stats*
 
 // Per-vertex triangle counts (each triangle adds 1 to each of its three
 // vertices) into d_tri (n zeroed counters, outside the scratch arena) under
-// the plan of `variant` (the matrix form has a per-vertex mode too).
-// Returns the triangle count.
+// the plan of `variant`; the matrix form has no per-vertex mode, so its units
+// run with the 32-lane bitmap kernel.  Returns the triangle count.
 pc_status tc_vertex_triangles(pc_pgraph* pg, int32_t variant, unsigned long long* d_tri, uint64_t* count) {
     PC_TRY(tc_ensure_features(pg));
     const size_t U = pg->unit_lo.size();
@@ -1059,6 +990,11 @@ pc_status tc_vertex_triangles(pc_pgraph* pg, int32_t variant, unsigned long long
     std::vector<int8_t> assign;
     int sel = 0;
     PC_TRY(tc_assign(pg, variant, pg->part_features, U, &assign, &sel));
+    for (size_t u = 0; u < U; ++u) {
+        if (assign[u] != PC_VARIANT_MATRIX) continue;
+        const float* f = &pg->part_features[u * kNumFeatures];
+        assign[u] = (int8_t)(bitmap_feasible(f) ? PC_VARIANT_BITMAP_WARP : PC_VARIANT_HASH_WARP);
+    }
     return tc_execute(pg, assign, count, nullptr, nullptr, d_tri);
 }
 

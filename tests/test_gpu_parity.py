@@ -321,7 +321,8 @@ def test_matrix_form_on_hub_units(gpu, O, scale, P):
         sel.set_heuristic([1.0, 48.0, 6.0, 0.0])  # matrix wherever it is feasible
         c, st = pg.triangle_count(variant=pc.VARIANT_HEURISTIC, stats=True)
         assert c == t and st.variant_hist[pc.VARIANTS["matrix"]] > 0
-        # the per-vertex mode of the matrix form (LCC), bit-exact with NaN at degree 1
+        # LCC under the same plan (matrix units run the 32-lane bitmap kernel in
+        # per-vertex mode), bit-exact with NaN at degree 1
         lcc = pg.solve_lcc_merge()
         want = O.lcc(vl, el)
         np.testing.assert_array_equal(np.isnan(lcc), np.isnan(want))
