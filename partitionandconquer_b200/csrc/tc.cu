@@ -633,62 +633,24 @@ static pc_status launch_matrix(pc_pgraph* pg, int64_t lo, int64_t hi, uint32_t h
     return PC_OK;
 }
 
-// Budget for the resident rows of one matrix launch: 32 MB by default (the
-// rows of a 16 K-pivot unit below id 16 K), PC_MATRIX_ROWS_MB in the
-// environment for measurements (0: the whole unit at once).  Rows beyond the
-// budget crowd the L2 the form relies on: at RMAT-24 the units of ids
-// 16-32 K and 32-48 K hold 64 and 96 MB of rows.
-static uint64_t matrix_rows_budget() {
-    static const uint64_t b = [] {
-        const char* e = getenv("PC_MATRIX_ROWS_MB");
-        const long v = e ? atol(e) : 32;
-        return v <= 0 ? UINT64_MAX : (uint64_t)v << 20;
-    }();
-    return b;
-}
-
-// The pivot slices [lo', hi') of a matrix unit [lo, hi) whose rows fit the
-// budget; each pair (b, c) of the unit belongs to the slice holding b, so the
-// slices' counts add up to the unit's.  Every slice reads the in-neighbours'
-// spans again, which costs far less than rows falling out of L2.
-static std::vector<std::pair<int64_t, int64_t>> matrix_slices(int64_t lo, int64_t hi) {
-    const uint64_t row = (uint64_t)matrix_stride(hi) * 4;
-    const uint64_t budget = matrix_rows_budget();
-    const int64_t rows = budget == UINT64_MAX ? hi - lo : (int64_t)std::max<uint64_t>(256, budget / row);
-    std::vector<std::pair<int64_t, int64_t>> out;
-    for (int64_t a = lo; a < hi; a += rows) out.emplace_back(a, std::min(hi, a + rows));
-    return out;
-}
-
-// Bytes of the rows of the largest slice of [lo, hi).
-static uint64_t matrix_slice_bytes(int64_t lo, int64_t hi) {
-    uint64_t b = 0;
-    for (const auto& sl : matrix_slices(lo, hi)) b = std::max(b, matrix_bytes(sl.first, sl.second));
-    return b;
-}
-
 // The in-neighbour-major form over one unit (ids [lo, hi)), all asynchronous:
-// per slice of pivots, rows H built from N+(b), then the walk over the
-// in-neighbours.
+// rows H built from N+(b), then the walk over the in-neighbours.
 static pc_status run_matrix_unit(pc_pgraph* pg, int64_t lo, int64_t hi, int32_t unit, uint32_t* H,
                                  unsigned long long* d_next, unsigned long long* d_total, unsigned long long* d_cost,
                                  uint64_t* launches) {
     cudaStream_t s = pg->g->stream;
     const int sms = sm_count(pg->g->device);
-    for (const auto& sl : matrix_slices(lo, hi)) {
-        const int64_t a = sl.first, b = sl.second;
-        const uint32_t hstride = matrix_stride(b);
-        PC_CUDA(cudaMemsetAsync(H, 0, matrix_bytes(a, b), s));
-        PC_CUDA(cudaMemsetAsync(d_next, 0, 16, s));
-        k_matrix_rows<<<sms * 8, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), (int32_t)a, (int32_t)b,
-                                              hstride, H);
-        PC_LAUNCHED();
-        if (matrix_pivot_block() == 8)
-            PC_TRY(launch_matrix<8>(pg, a, b, hstride, H, d_next, d_total, d_cost, unit, sms, s));
-        else
-            PC_TRY(launch_matrix<4>(pg, a, b, hstride, H, d_next, d_total, d_cost, unit, sms, s));
-        *launches += 2;
-    }
+    const uint32_t hstride = matrix_stride(hi);
+    PC_CUDA(cudaMemsetAsync(H, 0, matrix_bytes(lo, hi), s));
+    PC_CUDA(cudaMemsetAsync(d_next, 0, 16, s));
+    k_matrix_rows<<<sms * 8, 256, 0, s>>>(pg->off, pg->adj, pg->dplus.as<uint32_t>(), (int32_t)lo, (int32_t)hi, hstride,
+                                          H);
+    PC_LAUNCHED();
+    if (matrix_pivot_block() == 8)
+        PC_TRY(launch_matrix<8>(pg, lo, hi, hstride, H, d_next, d_total, d_cost, unit, sms, s));
+    else
+        PC_TRY(launch_matrix<4>(pg, lo, hi, hstride, H, d_next, d_total, d_cost, unit, sms, s));
+    *launches += 2;
     return PC_OK;
 }
 
@@ -704,7 +666,7 @@ static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long l
                            unsigned long long* d_cost, unsigned long long* d_tri, uint32_t* d_ecnt) {
     if (gr.v == PC_VARIANT_MATRIX) {
         uint64_t hb = 0;
-        for (size_t i = 0; i < gr.unit_ids.size(); ++i) hb = std::max(hb, matrix_slice_bytes(gr.ranges[2 * i], gr.ranges[2 * i + 1]));
+        for (size_t i = 0; i < gr.unit_ids.size(); ++i) hb = std::max(hb, matrix_bytes(gr.ranges[2 * i], gr.ranges[2 * i + 1]));
         uint32_t* H = pg->scratch.take<uint32_t>(hb / 4);
         unsigned long long* d_next = pg->scratch.take<unsigned long long>(2);
         if (!H || !d_next) return fail(PC_ERR_OOM, "scratch arena too small (internal sizing error)");
@@ -870,7 +832,7 @@ static pc_status tc_execute(pc_pgraph* pg, const std::vector<int8_t>& assign, ui
         if (gr.v == PC_VARIANT_MATRIX) {
             uint64_t hb = 0;
             for (size_t i = 0; i < gr.unit_ids.size(); ++i)
-                hb = std::max(hb, matrix_slice_bytes(gr.ranges[2 * i], gr.ranges[2 * i + 1]));
+                hb = std::max(hb, matrix_bytes(gr.ranges[2 * i], gr.ranges[2 * i + 1]));
             need += hb + 2 * 256;
             continue;
         }
