@@ -515,7 +515,9 @@ def run_ours(args, dist):
         pg.close()
         g.close()
         return
+    t_train = time.time()
     train = train_selector(pc, args)
+    t_train = time.time() - t_train
 
     g = pc.Graph(vlist=vl, elist=el)
     pg = pc.Partitioned_Graph(g, v2p)
@@ -572,7 +574,9 @@ def run_ours(args, dist):
     for a in pinned:
         L.lib.pc_host_unregister(L.ptr(a))
     bounds = plan_bounds(pc, pg)
+    t_cfg5 = time.time()
     cfg5 = learned_vs_plain_config5(pc, torch, args) if not args.no_config5 else None
+    t_cfg5 = time.time() - t_cfg5
     e2e_s = dist.max(statistics.median(e2e))
     e2e_value = dist.world * e_plus / e2e_s / 1e9
     h2d = vl.nbytes + el.nbytes + v2p.nbytes
@@ -619,7 +623,8 @@ def run_ours(args, dist):
             "cpu_baseline": cpu,
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
-            "setup": {"graph_gen_s": round(t_gen, 2)},
+            "setup": {"graph_gen_s": round(t_gen, 2), "selector_training_s": round(t_train, 1),
+                      "config5_s": round(t_cfg5, 1), "oracle_parity_s": parity["oracle_s"] if parity else None},
         }
         print(json.dumps(line), flush=True)
     pg.close()
