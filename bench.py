@@ -381,9 +381,10 @@ def train_selector(pc, args):
     at 2^20, and Chung-Lu at 2^20 (mean degree 8) and 2^22 (mean degree 32,
     as config 3's), all with other seeds than the measured graphs; each is
     partitioned into 16 K-vertex units like the measured graphs.  The
-    heuristic is autotuned on the samples, then the MLP is trained on the GPU
-    (each unit weighted by its time) with its judge margin chosen by
-    leave-one-graph-out validation."""
+    heuristic is autotuned on the samples (its best threshold sets by in-situ
+    unit costs, then timed as whole plans on two of the training graphs), then
+    the MLP is trained on the GPU (each unit weighted by its time) with its
+    judge margin chosen by leave-one-graph-out validation."""
     sel = pc.selector
     sel.clear()
     s = args.train_scale
@@ -395,17 +396,28 @@ def train_selector(pc, args):
               lambda: pc.Graph.er_device(s - 2, 1 << (s + 2), args.seed + 2),
               lambda: pc.Graph(host=pc.HostCSR.chung_lu(s - 2, 1 << (s + 2), 2.1, 1 << (s - 6), args.seed + 3)),
               lambda: pc.Graph(host=pc.HostCSR.chung_lu(s, 1 << (s + 4), 2.1, 1 << (s - 4), args.seed + 6))]
-    for make in graphs:
+    keep = {2, 3}  # RMAT-(s+2) and the first RMAT-25 verify the autotuner's candidates
+    kept = []
+    for i, make in enumerate(graphs):
         g = make()
         n = g.get_vertex_num()
         pg = pc.Partitioned_Graph(g, pc.equal_vertex_partition(n, max(1, n // 16384)))
         sel.collect_insitu(pg, repeats=2)
+        if i in keep:
+            kept.append((g, pg))
+        else:
+            pg.close()
+            g.close()
+    tuned, verify_ms = sel.autotune(verify=[pg for _, pg in kept], k=8, repeats=3)
+    for g, pg in kept:
         pg.close()
         g.close()
-    tuned = sel.autotune()
     loss = sel.train(steps=1500, lr=3e-3, seed=7)
     margin, gain = sel.judge()
     return {"samples": sel.num_samples(), "train_loss": loss, "heuristic_params": tuned.tolist(),
+            "autotune": f"8 best threshold sets by in-situ unit costs, and the defaults, timed on RMAT-{s + 2} "
+                        f"(seed {args.seed + 5}) and RMAT-25 (seed {args.seed + 1}): {round(verify_ms, 2)} ms summed "
+                        "for the kept set",
             "judge_margin": None if not np.isfinite(margin) else round(float(np.exp(margin)), 4),
             "heldout_gain_vs_plain": round(gain, 4),
             "training_graphs": f"RMAT-{s - 2}/{s}/{s + 2} and RMAT-25 x2 (seeds {args.seed + 4}, {args.seed + 1}, "

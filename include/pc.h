@@ -364,6 +364,14 @@ pc_status pc_selector_judge(double* log_margin, double* heldout_gain);
 pc_status pc_selector_predict(const float* feats, int32_t count, float* log_ms);
 /* Grid-search the heuristic's thresholds on the collected samples. */
 pc_status pc_selector_autotune(double* tuned /* 4 */);
+/* Two-stage autotuning: the k best threshold sets by the same grid search on
+ * the collected samples (distinct plans only), plus the thresholds in force,
+ * are each applied and timed on the npg graph views (the heuristic plan's
+ * counting time, median of `repeats` after one warm-up call); the set with
+ * the lowest summed time is kept and returned with that time.  The views
+ * should be graphs other than the ones the plan is measured on. */
+pc_status pc_selector_autotune_measured(pc_pgraph* const* pgs, int32_t npg, int32_t k, int32_t repeats,
+                                        double* tuned /* 4 */, double* measured_ms);
 /* Heuristic thresholds: in-edges per pivot for a shared-memory or resident
  * bitmap form; mean prefix length for 32 lanes, for 8 lanes, and for the
  * matrix form (1e30 = never). */

@@ -141,6 +141,7 @@ _SIG = {
     "pc_selector_train": (i32, [i32, f32, u64, P]),
     "pc_selector_predict": (i32, [P, i32, P]),
     "pc_selector_autotune": (i32, [P]),
+    "pc_selector_autotune_measured": (i32, [P, i32, i32, i32, P, P]),
     "pc_selector_get_heuristic": (i32, [P]),
     "pc_selector_set_heuristic": (i32, [P]),
     "pc_selector_clear": (i32, []),

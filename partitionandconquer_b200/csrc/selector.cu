@@ -917,8 +917,15 @@ pc_status pc_selector_set_heuristic(const double* p) {
 
 // Autotuner of the plain heuristic: grid search of its four thresholds that
 // minimises the summed measured time of its choices over the collected samples.
-pc_status pc_selector_autotune(double* tuned) {
-    clear_error();
+}  // extern "C"
+
+namespace pc {
+
+// Thresholds of the heuristic ranked by the proxy objective: the sum over all
+// collected samples of the in-situ cost of the variant the rule picks.  Grid
+// points that pick the same variants everywhere tie; the first of each total
+// (grid order) represents it.  Returns up to k distinct totals, best first.
+static pc_status autotune_rank(size_t k, std::vector<HeuristicParams>* out, std::vector<double>* proxy) {
     std::vector<float> feats, logms;
     std::vector<uint8_t> mask;
     {
@@ -931,8 +938,6 @@ pc_status pc_selector_autotune(double* tuned) {
     if (n == 0) return fail(PC_ERR_INVALID_INPUT, "no samples collected");
     const double grid_in[] = {1, 2, 4, 8, 16, 32, 64, 128, 256, 1e30};
     const double grid_scan[] = {0, 2, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 1e30};
-    HeuristicParams best = heuristic_params();
-    double best_t = 1e300;
     auto total = [&](const HeuristicParams& hp) {
         double t = 0;
         for (size_t s = 0; s < n; ++s) {
@@ -943,6 +948,7 @@ pc_status pc_selector_autotune(double* tuned) {
         }
         return t;
     };
+    std::vector<std::pair<double, HeuristicParams>> all;
     for (double a : grid_in)
         for (double w : grid_scan)
             for (double g : grid_scan) {
@@ -950,16 +956,93 @@ pc_status pc_selector_autotune(double* tuned) {
                 for (double mx : grid_scan) {
                     HeuristicParams hp{a, w, g, mx};
                     const double t = total(hp);
-                    if (t < best_t) { best_t = t; best = hp; }
+                    if (t < 1e299) all.emplace_back(t, hp);
                 }
             }
-    set_heuristic_params(best);
-    if (tuned) {
-        tuned[0] = best.min_in_per_pivot_cta;
-        tuned[1] = best.warp_scan;
-        tuned[2] = best.group_scan;
-        tuned[3] = best.matrix_scan;
+    std::stable_sort(all.begin(), all.end(),
+                     [](const std::pair<double, HeuristicParams>& x, const std::pair<double, HeuristicParams>& y) {
+                         return x.first < y.first;
+                     });
+    out->clear();
+    proxy->clear();
+    for (const auto& e : all) {
+        if (out->size() >= k) break;
+        if (!proxy->empty() && e.first == proxy->back()) continue;
+        out->push_back(e.second);
+        proxy->push_back(e.first);
     }
+    if (out->empty()) return fail(PC_ERR_INVALID_INPUT, "no threshold set can run every sample");
+    return PC_OK;
+}
+
+static void params_out(const HeuristicParams& hp, double* p) {
+    p[0] = hp.min_in_per_pivot_cta;
+    p[1] = hp.warp_scan;
+    p[2] = hp.group_scan;
+    p[3] = hp.matrix_scan;
+}
+
+}  // namespace pc
+
+extern "C" {
+
+pc_status pc_selector_autotune(double* tuned) {
+    clear_error();
+    std::vector<HeuristicParams> cand;
+    std::vector<double> proxy;
+    PC_TRY(autotune_rank(1, &cand, &proxy));
+    set_heuristic_params(cand[0]);
+    if (tuned) params_out(cand[0], tuned);
+    return PC_OK;
+}
+
+pc_status pc_selector_autotune_measured(pc_pgraph* const* pgs, int32_t npg, int32_t k, int32_t repeats,
+                                        double* tuned, double* measured_ms) {
+    clear_error();
+    if (!pgs || npg < 1 || k < 1 || repeats < 1) return fail(PC_ERR_INVALID_INPUT, "bad argument");
+    for (int32_t i = 0; i < npg; ++i)
+        if (!pgs[i]) return fail(PC_ERR_INVALID_INPUT, "null graph view");
+    std::vector<HeuristicParams> cand;
+    std::vector<double> proxy;
+    PC_TRY(autotune_rank((size_t)k, &cand, &proxy));
+    // the thresholds in force before tuning compete too
+    cand.push_back(heuristic_params());
+    const HeuristicParams before = heuristic_params();
+    double best_ms = INFINITY;
+    size_t best = 0;
+    for (size_t c = 0; c < cand.size(); ++c) {
+        set_heuristic_params(cand[c]);
+        double sum = 0;
+        for (int32_t i = 0; i < npg; ++i) {
+            PC_TRY(use_device(pgs[i]->g));
+            std::vector<double> t;
+            uint64_t cnt0 = 0;
+            for (int32_t r = 0; r <= repeats; ++r) {  // the first call plans and warms up
+                uint64_t cnt = 0;
+                pc_tc_stats st;
+                const pc_status e = tc_count(pgs[i], PC_VARIANT_HEURISTIC, &cnt, &st);
+                if (e != PC_OK) {
+                    set_heuristic_params(before);
+                    return e;
+                }
+                if (r == 0) cnt0 = cnt;
+                else t.push_back(st.kernel_ms);
+                if (cnt != cnt0) {
+                    set_heuristic_params(before);
+                    return fail(PC_ERR_INVALID_INPUT, "autotune: counts differ between calls");
+                }
+            }
+            std::sort(t.begin(), t.end());
+            sum += t[t.size() / 2];
+        }
+        if (sum < best_ms) {
+            best_ms = sum;
+            best = c;
+        }
+    }
+    set_heuristic_params(cand[best]);
+    if (tuned) params_out(cand[best], tuned);
+    if (measured_ms) *measured_ms = best_ms;
     return PC_OK;
 }
 

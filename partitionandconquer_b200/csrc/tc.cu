@@ -3,6 +3,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <initializer_list>
 #include <cmath>
 #include <cstring>
 
@@ -215,21 +216,21 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// A warp-private stage holds up to kStageIds ids of a span: the copy starts
+// A warp-private stage holds up to kStageIds ids of a span (or the smaller
+// stage a launch chooses, svec uint4): the copy starts
 // at the 16-byte boundary at or below the span (up to 3 ids early) and may
 // end up to 3 ids past it, which the 64 ids of padding after the last row
 // keep inside the adjacency array.
 constexpr uint32_t kStageIds = 512;
-constexpr uint32_t kStageVec = kStageIds / 4 + 1;  // uint4 per stage (span + up to 3 leading ids)
 
 // Issues the copies of ids [r, r + k) of adj into stage; returns the offset
 // of id r inside it, or -1 when the span does not fit (it is then read from
 // global memory).
 __device__ __forceinline__ int stage_span(const int32_t* __restrict__ adj, uint64_t r, uint32_t k, uint4* stage,
-                                          int lane) {
+                                          uint32_t svec, int lane) {
     const uint32_t shift = (uint32_t)(r & 3);
     const uint32_t nvec = (shift + k + 3) >> 2;
-    if (nvec > kStageVec) return -1;
+    if (nvec > svec) return -1;
     const uint4* src = reinterpret_cast<const uint4*>(adj + (r - shift));
     for (uint32_t x = lane; x < nvec; x += 32) cp_async16(stage + x, src + x);
     return (int)shift;
@@ -342,11 +343,12 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
                                                                unsigned long long* __restrict__ next,
                                                                unsigned long long* __restrict__ total,
                                                                unsigned long long* __restrict__ unit_cost,
-                                                               int32_t unit) {
+                                                               int32_t unit, uint32_t svec) {
     extern __shared__ uint4 msm4[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t nwarps = blockDim.x >> 5;  // kMatrixWarps or fewer
     uint32_t* Sb = reinterpret_cast<uint32_t*>(msm4) + (size_t)w * hstride;  // warp-private bitmap of S_c
-    uint4* stage = msm4 + (size_t)kMatrixWarps * (hstride / 4) + (size_t)w * 2 * kStageVec;
+    uint4* stage = msm4 + (size_t)nwarps * (hstride / 4) + (size_t)w * 2 * svec;
     for (uint32_t i = lane; i < hstride; i += 32) Sb[i] = 0;
     __syncwarp();
     const long long t0 = unit_cost ? clock64() : 0;
@@ -380,7 +382,7 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
         todo &= todo - 1;
         int buf = 0;
         int shift = stage_span(adj, __shfl_sync(0xffffffffu, r, src), __shfl_sync(0xffffffffu, khi, src),
-                               stage, lane);
+                               stage, svec, lane);
         cp_async_commit();
         for (;;) {
             const int nxt = todo ? __ffs(todo) - 1 : -1;
@@ -388,14 +390,14 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
             int nshift = -1;
             if (nxt >= 0)
                 nshift = stage_span(adj, __shfl_sync(0xffffffffu, r, nxt), __shfl_sync(0xffffffffu, khi, nxt),
-                                    stage + (buf ^ 1) * kStageVec, lane);
+                                    stage + (buf ^ 1) * svec, svec, lane);
             cp_async_commit();
             cp_async_wait<1>();  // every group but the one just issued: the current span is in place
             __syncwarp();
             const uint64_t rs = __shfl_sync(0xffffffffu, r, src);
             const uint32_t j0 = __shfl_sync(0xffffffffu, klo, src);
             const uint32_t k = __shfl_sync(0xffffffffu, khi, src);
-            const int32_t* S = shift >= 0 ? reinterpret_cast<const int32_t*>(stage + buf * kStageVec) + shift
+            const int32_t* S = shift >= 0 ? reinterpret_cast<const int32_t*>(stage + buf * svec) + shift
                                           : adj + rs;
             cnt += matrix_block_pairs<U>(S, j0, k, lo, hstride, H, Sb, lane);
             __syncwarp();  // the buffer just read is the next stage's target
@@ -503,14 +505,22 @@ struct BitmapLaunch {
     uint32_t* ecnt;           // per-edge counts at the oriented slots (Jaccard), or null
 };
 
-template <int K, int G, bool kVC, bool kEC>
+template <int K, int G, bool kVC, bool kEC, bool kSplit = false>
 static pc_status launch_bitmap_kgv(const BitmapLaunch& L) {
-    PC_CUDA(cudaFuncSetAttribute(k_tc_bitmap<K, G, kVC, kEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    PC_CUDA(cudaFuncSetAttribute(k_tc_bitmap<K, G, kVC, kEC, kSplit>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)L.smem));
-    k_tc_bitmap<K, G, kVC, kEC><<<L.grid, kCtaThreads, L.smem, L.s>>>(L.off, L.adj, L.dp, L.plist, L.items, L.nitems,
-                                                                    L.next, L.total, L.words, L.cost, L.unit_of,
-                                                                    L.tri, L.ecnt);
+    k_tc_bitmap<K, G, kVC, kEC, kSplit><<<L.grid, kCtaThreads, L.smem, L.s>>>(
+        L.off, L.adj, L.dp, L.plist, L.items, L.nitems, L.next, L.total, L.words, L.cost, L.unit_of, L.tri, L.ecnt);
     return PC_OK;
+}
+
+// Split-set launches (count mode): sets of kSplitWords + kHashSlots words
+// (10 KB), so bitmap_shape gives K = 2 for every such launch.
+static pc_status launch_bitmap_split(int K, int G, const BitmapLaunch& L) {
+    if (K != 2 || L.tri || L.ecnt) return fail(PC_ERR_UNSUPPORTED, "split pivot sets: unexpected launch shape");
+    if (G == 32) return launch_bitmap_kgv<2, 32, false, false, true>(L);
+    if (G == 8) return launch_bitmap_kgv<2, 8, false, false, true>(L);
+    return launch_bitmap_kgv<2, 1, false, false, true>(L);
 }
 
 template <int K, bool kVC, bool kEC>
@@ -594,6 +604,7 @@ pc_status tc_ensure_features(pc_pgraph* pg) {
 struct LaunchGroup {
     int v = -1;
     uint32_t words = 0;
+    bool split = false;  // bitmap variants: SplitSets (kSplitWords bitmap words + a hash)
     std::vector<int64_t> ranges;
     uint64_t npos = 0, item_bound = 0;
     double ein = 0;
@@ -608,6 +619,17 @@ static uint32_t matrix_stride(int64_t hi) { return (uint32_t)((((hi + 31) / 32) 
 // Bytes of the resident pivot bitmap rows of a matrix unit [lo, hi).
 static uint64_t matrix_bytes(int64_t lo, int64_t hi) { return (uint64_t)(hi - lo) * matrix_stride(hi) * 4; }
 
+// Bitmap units whose pivot ids reach kSplitLo or more run with SplitSets in
+// the count mode, unless PC_BITMAP_SPLIT=0 is in the environment (read once;
+// a switch for measurements).
+static bool bitmap_split_enabled() {
+    static const bool on = [] {
+        const char* e = getenv("PC_BITMAP_SPLIT");
+        return !(e && atoi(e) == 0);
+    }();
+    return on;
+}
+
 // Pivots per block of the matrix kernel: 4, or 8 with PC_MATRIX_PIVOT_BLOCK=8
 // in the environment (read once; a tuning override for measurements).
 static int matrix_pivot_block() {
@@ -618,17 +640,39 @@ static int matrix_pivot_block() {
     return u;
 }
 
+// Matrix launch shape: warps per CTA (kMatrixWarps, or PC_MATRIX_WARPS=4) and
+// ids per span stage (kStageIds, or PC_MATRIX_STAGE_IDS=128|256|1024), read
+// once from the environment; switches for measurements.
+static int matrix_env(const char* name, int dflt, std::initializer_list<int> allowed) {
+    const char* e = getenv(name);
+    if (!e) return dflt;
+    const int v = atoi(e);
+    for (int a : allowed)
+        if (a == v) return v;
+    return dflt;
+}
+static int matrix_warps() {
+    static const int w = matrix_env("PC_MATRIX_WARPS", kMatrixWarps, {4, 8});
+    return w;
+}
+static uint32_t matrix_stage_vec() {
+    static const uint32_t v = (uint32_t)matrix_env("PC_MATRIX_STAGE_IDS", (int)kStageIds, {128, 256, 512, 1024}) / 4 + 1;
+    return v;
+}
+
 template <int U>
 static pc_status launch_matrix(pc_pgraph* pg, int64_t lo, int64_t hi, uint32_t hstride, const uint32_t* H,
                                unsigned long long* d_next, unsigned long long* d_total, unsigned long long* d_cost,
                                int32_t unit, int sms, cudaStream_t s) {
-    const size_t smem = (size_t)kMatrixWarps * hstride * 4 + (size_t)kMatrixWarps * 2 * kStageVec * sizeof(uint4);
+    const int warps = matrix_warps();
+    const uint32_t svec = matrix_stage_vec();
+    const size_t smem = (size_t)warps * hstride * 4 + (size_t)warps * 2 * svec * sizeof(uint4);
     PC_CUDA(cudaFuncSetAttribute(k_tc_matrix<U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    PC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_matrix<U>, kMatrixWarps * 32, smem));
-    k_tc_matrix<U><<<(unsigned)(sms * std::max(1, per_sm)), kMatrixWarps * 32, smem, s>>>(
+    PC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_matrix<U>, warps * 32, smem));
+    k_tc_matrix<U><<<(unsigned)(sms * std::max(1, per_sm)), warps * 32, smem, s>>>(
         pg->off, pg->adj, pg->dplus.as<uint32_t>(), (int32_t)lo, (int32_t)hi, pg->g->n, hstride, H, d_next, d_total,
-        d_cost, unit);
+        d_cost, unit, svec);
     PC_LAUNCHED();
     return PC_OK;
 }
@@ -690,7 +734,7 @@ static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long l
     int64_t* d_pref = nullptr;
     PC_TRY(upload(pg, gr.ranges.data(), gr.ranges.size(), &d_ranges));
     PC_TRY(upload(pg, pref.data(), nr + 1, &d_pref));
-    const BitmapShape sh = bitmap_shape(gr.words * 32u);
+    const BitmapShape sh = bitmap_shape((gr.split ? kSplitWords + (uint32_t)kHashSlots : gr.words) * 32u);
     const uint32_t chunk = is_bitmap(v) ? 256u * (uint32_t)sh.K : (uint32_t)kChunkWarp;
     uint32_t* d_cnt = pg->scratch.take<uint32_t>(npos + 1);
     uint32_t* d_start = pg->scratch.take<uint32_t>(npos + 1);
@@ -731,13 +775,14 @@ static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long l
         L.nitems = d_nitems;
         L.next = d_next;
         L.total = d_total;
-        L.words = sh.words;
+        L.words = gr.split ? kSplitWords : sh.words;
         L.cost = d_cost;
         L.unit_of = unit_of;
         L.tri = d_tri;
         L.ecnt = d_ecnt;
         const int Gsel = v == PC_VARIANT_BITMAP_WARP ? 32 : (v == PC_VARIANT_BITMAP_GROUP8 ? 8 : 1);
-        PC_TRY(launch_bitmap(sh.K, Gsel, L));
+        if (gr.split) PC_TRY(launch_bitmap_split(sh.K, Gsel, L));
+        else PC_TRY(launch_bitmap(sh.K, Gsel, L));
     } else {
         const unsigned grid = (unsigned)std::max<uint64_t>(
             1, std::min<uint64_t>((uint64_t)sms * 8, ceil_div(gr.item_bound, kWarpCtaWarps)));
@@ -795,9 +840,12 @@ static pc_status tc_execute(pc_pgraph* pg, const std::vector<int8_t>& assign, ui
     const std::vector<float>& feat = pg->part_features;
     const size_t U = lo.size();
     // Bitmap units are grouped by their bitmap size rounded up to a power of
-    // two, so the hub units (small ids) get small sets and more CTAs per SM.
+    // two, so the hub units (small ids) get small sets and more CTAs per SM;
+    // in the count mode, units with pivot ids past kSplitLo share one group of
+    // fixed-size SplitSets (class kClasses).
     constexpr int kClasses = 16;
-    std::vector<LaunchGroup> groups(PC_NUM_VARIANTS * kClasses);
+    const bool split_ok = bitmap_split_enabled() && !d_tri && !d_ecnt;
+    std::vector<LaunchGroup> groups(PC_NUM_VARIANTS * (kClasses + 1));
     std::vector<int> group_of(U, -1);
     for (size_t u = 0; u < U; ++u) {
         const int v = assign[u];
@@ -807,11 +855,13 @@ static pc_status tc_execute(pc_pgraph* pg, const std::vector<int8_t>& assign, ui
         if (is_bitmap(v)) {
             const uint32_t w = std::max<uint32_t>(1, (mid + 31) / 32);
             while ((1u << c) < w && c < kClasses - 1) ++c;
+            if (split_ok && mid > (uint32_t)kSplitLo) c = kClasses;
         }
-        LaunchGroup& gr = groups[v * kClasses + c];
-        group_of[u] = v * kClasses + c;
+        LaunchGroup& gr = groups[v * (kClasses + 1) + c];
+        group_of[u] = v * (kClasses + 1) + c;
         gr.v = v;
-        gr.words = 1u << c;
+        gr.split = c == kClasses;
+        gr.words = gr.split ? kSplitWords : 1u << c;
         if (v == PC_VARIANT_MATRIX) {
             gr.ranges.push_back(lo[u]);
             gr.ranges.push_back(hi[u]);

@@ -22,6 +22,8 @@
 #pragma once
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "pc_internal.cuh"
 
 namespace pc {
@@ -47,6 +49,49 @@ struct Item {
 __device__ __forceinline__ int32_t pivot_at(const int32_t* __restrict__ plist, int64_t p) {
     return plist ? plist[p] : (int32_t)p;
 }
+
+__device__ __forceinline__ uint32_t hash_slot(int32_t a) { return ((uint32_t)a * 0x9E3779B1u) >> (32 - 9); }
+
+// Pivot sets the bitmap kernels test prefix ids against.
+//
+// BitmapSet: bit a of a shared-memory bitmap for every a in N+(b).
+//
+// SplitSet: ids below kSplitLo in a bitmap of kSplitLo bits (8 KB), ids at or
+// above it in a 512-slot open-addressing hash.  The set's size no longer
+// grows with the pivot's id, so units of pivots up to 2^20 keep 8 sets per
+// CTA.  A pivot with more than kHashCap ids at or above kSplitLo does not fill
+// the hash; its high ids are then found by binary search in N+(b) itself
+// (`ovf`), so the test stays exact for every pivot.
+constexpr int32_t kSplitLo = 1 << 16;
+constexpr uint32_t kSplitWords = (uint32_t)kSplitLo / 32;
+
+struct BitmapSet {
+    const uint32_t* bm;
+    __device__ __forceinline__ uint32_t test(int32_t a) const { return (bm[a >> 5] >> (a & 31)) & 1u; }
+};
+
+struct SplitSet {
+    const uint32_t* bm;
+    const int32_t* ht;             // kHashSlots slots, -1 = empty
+    const int32_t* __restrict__ nb;  // N+(b) in the CSR (overflow path)
+    uint32_t dp;
+    bool ovf;
+    __device__ __forceinline__ uint32_t test(int32_t a) const {
+        if (a < kSplitLo) return (bm[a >> 5] >> (a & 31)) & 1u;
+        if (ovf) {
+            uint32_t lo = 0, hi = dp;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (__ldg(nb + mid) < a) lo = mid + 1; else hi = mid;
+            }
+            return (lo < dp && __ldg(nb + lo) == a) ? 1u : 0u;
+        }
+        uint32_t s = hash_slot(a);
+        for (int32_t key; (key = ht[s]) != -1; s = (s + 1) & (kHashSlots - 1))
+            if (key == a) return 1u;
+        return 0u;
+    }
+};
 
 // Group-of-G scan of the prefix N(c) & [0, b): the G lanes of a group read G
 // consecutive ids per step (coalesced) and test them against the pivot set.
@@ -101,10 +146,9 @@ __device__ __forceinline__ uint32_t rank_in_set(const uint32_t* __restrict__ bm,
 // triangle a < b < c adds 1 to the slot of a in row c (its scan index), to
 // the slot of a in row b (its rank in the pivot set) and, once per pair,
 // its hits to the slot of b in row c (where the scan stops).
-template <int G, bool kVC = false, bool kEC = false>
+template <int G, bool kVC = false, bool kEC = false, class Set = BitmapSet>
 __device__ __forceinline__ uint32_t scan_prefix_pipelined(const int32_t* __restrict__ row, uint32_t lim, int32_t b,
-                                                          int gl, unsigned gmask,
-                                                          const uint32_t* __restrict__ bm,
+                                                          int gl, unsigned gmask, const Set& S,
                                                           unsigned long long* __restrict__ tri = nullptr,
                                                           uint32_t* hist = nullptr,
                                                           uint32_t* __restrict__ ec_c = nullptr,
@@ -118,12 +162,12 @@ __device__ __forceinline__ uint32_t scan_prefix_pipelined(const int32_t* __restr
         const uint32_t inext = i + G;
         const int32_t an = inext < lim ? __ldg(row + inext) : 0x7fffffff;
         if (a < b) {
-            const uint32_t bit = (bm[a >> 5] >> (a & 31)) & 1u;
+            const uint32_t bit = S.test(a);
             hits += bit;
             if (kVC && bit) count_vertex(a, tri, hist);
             if (kEC && bit) {
                 atomicAdd(&ec_c[i], 1u);
-                atomicAdd(&ec_b[rank_in_set(bm, sb, a)], 1u);
+                atomicAdd(&ec_b[rank_in_set(S.bm, sb, a)], 1u);
             }
         } else if (kEC && a == b) {
             kb = (int32_t)i;
@@ -148,9 +192,9 @@ __device__ __forceinline__ uint32_t scan_prefix_pipelined(const int32_t* __restr
 // 16-byte boundary at or below its start (positions before 0 are masked);
 // a load may run up to 3 ids past lim, which the adjacency array's padding
 // (64 ids after the last row) keeps in bounds.
-template <int G, bool kVC = false, bool kEC = false>
+template <int G, bool kVC = false, bool kEC = false, class Set = BitmapSet>
 __device__ __forceinline__ uint32_t scan_prefix_vec4(const int32_t* __restrict__ row, uint32_t lim, int32_t b, int gl,
-                                                     unsigned gmask, const uint32_t* __restrict__ bm,
+                                                     unsigned gmask, const Set& S,
                                                      unsigned long long* __restrict__ tri = nullptr,
                                                      uint32_t* hist = nullptr, uint32_t* __restrict__ ec_c = nullptr,
                                                      uint32_t* __restrict__ ec_b = nullptr,
@@ -175,12 +219,12 @@ __device__ __forceinline__ uint32_t scan_prefix_vec4(const int32_t* __restrict__
             if (pos < 0 || pos >= (int64_t)lim) continue;
             const int32_t a = e[t];
             if (a < b) {
-                const uint32_t bit = (bm[a >> 5] >> (a & 31)) & 1u;
+                const uint32_t bit = S.test(a);
                 hits += bit;
                 if (kVC && bit) count_vertex(a, tri, hist);
                 if (kEC && bit) {
                     atomicAdd(&ec_c[pos], 1u);
-                    atomicAdd(&ec_b[rank_in_set(bm, sb, a)], 1u);
+                    atomicAdd(&ec_b[rank_in_set(S.bm, sb, a)], 1u);
                 }
             } else {
                 stop = true;
@@ -202,25 +246,28 @@ __device__ __forceinline__ uint32_t scan_prefix_vec4(const int32_t* __restrict__
 }
 
 // The prefix scan a group of G lanes runs: 16-byte loads below 32 lanes.
-template <int G, bool kVC = false, bool kEC = false>
+template <int G, bool kVC = false, bool kEC = false, class Set = BitmapSet>
 __device__ __forceinline__ uint32_t scan_group_prefix(const int32_t* __restrict__ row, uint32_t lim, int32_t b, int gl,
-                                                      unsigned gmask, const uint32_t* __restrict__ bm,
+                                                      unsigned gmask, const Set& S,
                                                       unsigned long long* __restrict__ tri = nullptr,
                                                       uint32_t* hist = nullptr, uint32_t* __restrict__ ec_c = nullptr,
                                                       uint32_t* __restrict__ ec_b = nullptr,
                                                       const uint32_t* __restrict__ sb = nullptr) {
-    if constexpr (G < 32) return scan_prefix_vec4<G, kVC, kEC>(row, lim, b, gl, gmask, bm, tri, hist, ec_c, ec_b, sb);
-    else return scan_prefix_pipelined<G, kVC, kEC>(row, lim, b, gl, gmask, bm, tri, hist, ec_c, ec_b, sb);
+    if constexpr (G < 32) return scan_prefix_vec4<G, kVC, kEC>(row, lim, b, gl, gmask, S, tri, hist, ec_c, ec_b, sb);
+    else return scan_prefix_pipelined<G, kVC, kEC>(row, lim, b, gl, gmask, S, tri, hist, ec_c, ec_b, sb);
 }
 
-// Bitmap kernel: a CTA of kCtaThreads threads holds 16/K pivot bitmaps in
+// Bitmap kernel: a CTA of kCtaThreads threads holds 16/K pivot sets in
 // shared memory, one per group of K warps; each group takes its own work
 // items (pivot, a run of its in-neighbours), so a group synchronises only
 // with itself (a named barrier, or nothing when K == 1).  In-neighbour metadata
 // (id, row offset, prefix length) is fetched 32 at a time with one coalesced
 // load and 32 independent gathers, then handed to groups of G lanes by
-// shuffles; each group scans one prefix with scan_prefix_pipelined.
-template <int K, int G, bool kVC = false, bool kEC = false>
+// shuffles; each group scans one prefix with scan_group_prefix.
+// With kSplit the sets are SplitSets: bm_words = kSplitWords bitmap words,
+// then kHashSlots hash slots, whatever the pivots' ids (count and per-vertex
+// modes; the per-edge mode needs ranks in a plain bitmap).
+template <int K, int G, bool kVC = false, bool kEC = false, bool kSplit = false>
 __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __restrict__ off,
                                                            const int32_t* __restrict__ adj,
                                                            const uint32_t* __restrict__ dplus,
@@ -234,14 +281,18 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
                                                            const int32_t* __restrict__ unit_of,
                                                            unsigned long long* __restrict__ tri = nullptr,
                                                            uint32_t* __restrict__ ecnt = nullptr) {
+    static_assert(!(kSplit && kEC), "per-edge counts need the plain bitmap's ranks");
     extern __shared__ uint32_t smem[];
     __shared__ uint32_t s_item[16];
+    __shared__ uint32_t s_hic[16];  // kSplit: ids >= kSplitLo offered to the set's hash this item
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int set = warp / K, wi = warp % K;
     const int nsets = (kCtaThreads / 32) / K;
     const int set_threads = K * 32, tis = wi * 32 + lane;
-    uint32_t* bm = smem + (size_t)set * bm_words;
-    uint32_t* hist = smem + (size_t)nsets * bm_words;  // kVC: kHubHist counters after the sets
+    const uint32_t set_words = bm_words + (kSplit ? (uint32_t)kHashSlots : 0u);
+    uint32_t* bm = smem + (size_t)set * set_words;
+    int32_t* ht = reinterpret_cast<int32_t*>(bm + bm_words);  // kSplit: the set's hash slots
+    uint32_t* hist = smem + (size_t)nsets * set_words;  // kVC: kHubHist counters after the sets
     // kEC: per set, the rank of the first pivot-set entry of every touched
     // 256-id superblock (only those are ever read)
     const uint32_t nsb = (bm_words + 7) / 8;
@@ -249,11 +300,13 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
     // kEC: per set, hits by rank in the pivot set (sets up to kEcRankCap),
     // flushed to the row's slots once per item
     uint32_t* ecs = smem + (size_t)nsets * (bm_words + nsb) + (size_t)set * kEcRankCap;
-    const uint32_t zero_words = (uint32_t)nsets * bm_words + (kVC ? (uint32_t)kHubHist : 0u);
-    for (uint32_t i = tid; i < zero_words; i += blockDim.x) smem[i] = 0;
+    const uint32_t zero_words = (uint32_t)nsets * set_words + (kVC ? (uint32_t)kHubHist : 0u);
+    for (uint32_t i = tid; i < zero_words; i += blockDim.x)
+        smem[i] = (kSplit && i < (uint32_t)nsets * set_words && i % set_words >= bm_words) ? 0xffffffffu : 0u;
     if (kEC)
         for (uint32_t i = tid; i < (uint32_t)nsets * kEcRankCap; i += blockDim.x)
             smem[(size_t)nsets * (bm_words + nsb) + i] = 0;
+    if (tid < 16) s_hic[tid] = 0;
     __syncthreads();
     auto set_sync = [&]() {
         if constexpr (K == 1) __syncwarp();
@@ -276,10 +329,20 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
         const uint32_t dp = dplus[b];
         for (uint32_t k = tis; k < dp; k += set_threads) {
             const int32_t a = adj[rb + k];
-            atomicOr(&bm[a >> 5], 1u << (a & 31));
+            if (!kSplit || a < kSplitLo) {
+                atomicOr(&bm[a >> 5], 1u << (a & 31));
+            } else if (atomicAdd(&s_hic[set], 1u) < (uint32_t)kHashCap) {
+                // at most kHashCap keys in kHashSlots slots: a free slot exists
+                uint32_t hs = hash_slot(a);
+                while (atomicCAS(&ht[hs], -1, a) != -1) hs = (hs + 1) & (kHashSlots - 1);
+            }
             if (kEC && (k == 0 || (adj[rb + k - 1] >> 8) != (a >> 8))) sb[a >> 8] = k;
         }
         set_sync();
+        const uint32_t hic = kSplit ? s_hic[set] : 0u;
+        std::conditional_t<kSplit, SplitSet, BitmapSet> S;
+        if constexpr (kSplit) S = SplitSet{bm, ht, adj + rb, dp, hic > (uint32_t)kHashCap};
+        else S = BitmapSet{bm};
         const uint64_t in0 = rb + dp + (uint64_t)I.j0;
         const uint64_t in1 = min(rb + dp + (uint64_t)I.j1, re);
         unsigned long long hb = 0;  // kVC: this item's triangles at pivot b
@@ -299,19 +362,19 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
                 uint32_t limj = __shfl_sync(0xffffffffu, lim, src);
                 if (j >= nb) limj = 0;
                 if (kEC) {
-                    if (limj) cnt += scan_group_prefix<G, false, true>(adj + rcj, limj, b, gl, gmask, bm, nullptr,
+                    if (limj) cnt += scan_group_prefix<G, false, true>(adj + rcj, limj, b, gl, gmask, S, nullptr,
                                                                            nullptr, ecnt + rcj,
                                                                            dp <= kEcRankCap ? ecs : ecnt + rb, sb);
                 } else if (kVC) {
                     const int32_t cj = __shfl_sync(0xffffffffu, c, src);
                     if (limj) {
-                        const uint32_t h = scan_group_prefix<G, true>(adj + rcj, limj, b, gl, gmask, bm, tri, hist);
+                        const uint32_t h = scan_group_prefix<G, true>(adj + rcj, limj, b, gl, gmask, S, tri, hist);
                         cnt += h;
                         hb += h;
                         if (h) atomicAdd(&tri[cj], (unsigned long long)h);
                     }
                 } else if (limj) {
-                    cnt += scan_group_prefix<G>(adj + rcj, limj, b, gl, gmask, bm);
+                    cnt += scan_group_prefix<G>(adj + rcj, limj, b, gl, gmask, S);
                 }
             }
         }
@@ -321,7 +384,8 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
         }
         set_sync();
         for (uint32_t k = tis; k < dp; k += set_threads) {
-            bm[adj[rb + k] >> 5] = 0;
+            const int32_t a = adj[rb + k];
+            if (!kSplit || a < kSplitLo) bm[a >> 5] = 0;
             if (kEC && dp <= kEcRankCap) {
                 const uint32_t h = ecs[k];
                 if (h) {
@@ -329,6 +393,10 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
                     ecs[k] = 0;
                 }
             }
+        }
+        if (kSplit && hic) {
+            for (uint32_t x = tis; x < (uint32_t)kHashSlots; x += set_threads) ht[x] = -1;
+            if (tis == 0) s_hic[set] = 0;  // every lane read it before the scan barrier
         }
         set_sync();
         // profiling runs: the set's warp-cycles on this item, charged to its unit
@@ -342,8 +410,6 @@ __global__ void __launch_bounds__(kCtaThreads) k_tc_bitmap(const uint64_t* __res
             if (hist[i]) atomicAdd(&tri[i], (unsigned long long)hist[i]);
     }
 }
-
-__device__ __forceinline__ uint32_t hash_slot(int32_t a) { return ((uint32_t)a * 0x9E3779B1u) >> (32 - 9); }
 
 // |x & y & [0, thr)| for sorted x, y: Partitioned_Graph::
 // cnt_common_neis_less_than_merge (src/Graph.cpp:1132-1153), without its

@@ -96,10 +96,19 @@ def predict(feats) -> np.ndarray:
     return out
 
 
-def autotune() -> np.ndarray:
+def autotune(verify=None, k: int = 8, repeats: int = 3):
+    """Heuristic thresholds from the collected samples.  With `verify` (graph
+    views other than the measured ones), the k best sets by the samples and
+    the thresholds in force are timed there and the fastest is kept; returns
+    (thresholds, summed ms).  Without, returns the samples' best thresholds."""
     out = np.empty(4, np.float64)
-    check(lib.pc_selector_autotune(ptr(out)))
-    return out
+    if not verify:
+        check(lib.pc_selector_autotune(ptr(out)))
+        return out
+    handles = (C.c_void_p * len(verify))(*[pg.handle for pg in verify])
+    ms = C.c_double()
+    check(lib.pc_selector_autotune_measured(handles, len(verify), k, repeats, ptr(out), C.byref(ms)))
+    return out, float(ms.value)
 
 
 def get_heuristic() -> np.ndarray:

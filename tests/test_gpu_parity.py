@@ -348,9 +348,11 @@ def test_matrix_form_on_hub_units(gpu, O, scale, P):
 
 
 def test_bitmap_kernels_every_set_shape(gpu, O):
-    """Forced bitmap variants on RMAT-20 with 64 partitions: pivot ids up to
-    2^20 make the kernels share one bitmap among K = 1, 2, 4, 8 and 16 warps
-    (named barriers) across the units; the count must not change."""
+    """Forced bitmap variants on RMAT-20 with 64 partitions.  In the count
+    mode units with pivot ids past 2^16 hold split sets (K = 2); in the
+    per-vertex mode (LCC) pivot ids up to 2^20 make the kernels share one
+    plain bitmap among K = 1, 2, 4, 8 and 16 warps (named barriers) across the
+    units.  Counts and LCC must equal the oracle's."""
     pc = gpu
     h = pc.HostCSR.rmat(20, 16, 5)
     vl, el, _ = h.arrays()
@@ -363,3 +365,68 @@ def test_bitmap_kernels_every_set_shape(gpu, O):
     f = pc.selector.unit_features(pg)
     assert f[:, 1].sum() == el.size // 2  # every in-edge belongs to one unit
     assert (f[:, 0].sum(), f[:, 4].max()) == (n, n)
+    # per-vertex mode (LCC) keeps the plain bitmaps of every size: a plan with
+    # the 8-lane bitmap kernel wherever it is feasible shares one set among
+    # K = 1 ... 16 warps across the units
+    saved = pc.selector.get_heuristic()
+    try:
+        pc.selector.set_heuristic([0.0, 1e9, 0.0, 1e9])
+        lcc = pg.solve_lcc_merge()
+    finally:
+        pc.selector.set_heuristic(saved)
+    want = O.lcc(vl, el)
+    np.testing.assert_array_equal(np.isnan(lcc), np.isnan(want))
+    np.testing.assert_array_equal(lcc, want)
+
+
+def _split_overflow_graph():
+    """Pivot ids past 2^16, where the count mode's bitmap kernels hold a pivot
+    set as a bitmap of the ids below 2^16 plus a 512-slot hash of the rest:
+    pivot b1 has 600 neighbours in [2^16, b1) (more than the hash takes, so
+    its high ids are found by binary search), pivot b2 has 100 (hashed); both
+    have 50 in-neighbours c > b whose rows hit random low and high ids of the
+    pivot's set."""
+    rng = np.random.default_rng(77)
+    L = 1 << 16
+    high = np.arange(L, L + 600)
+    low = np.arange(0, 100)
+    b1, b2 = L + 700, L + 760
+    edges = [(b1, int(x)) for x in high] + [(b1, int(x)) for x in low]
+    edges += [(b2, int(x)) for x in high[:100]] + [(b2, int(x)) for x in low[:40]]
+    for c in range(L + 800, L + 850):
+        edges.append((c, b1))
+        edges += [(c, int(x)) for x in rng.choice(np.concatenate([low, high]), 200, replace=False)]
+    for c in range(L + 900, L + 950):
+        edges.append((c, b2))
+        edges += [(c, int(x)) for x in rng.choice(np.concatenate([low[:60], high[:150]]), 60, replace=False)]
+    # some triangles among the high ids themselves
+    for i in range(0, 590, 7):
+        edges.append((int(high[i]), int(high[i + 3])))
+        edges.append((int(high[i]), int(low[i % 100])))
+        edges.append((int(high[i + 3]), int(low[i % 100])))
+    from conftest import csr_from_edges
+    return csr_from_edges(L + 1000, edges)
+
+
+def test_split_pivot_sets(gpu, O):
+    """Forced bitmap variants where pivot ids exceed 2^16: RMAT-18 with 16
+    partitions, and a graph whose pivot sets overflow the split set's hash;
+    the counts equal the oracle's."""
+    pc = gpu
+    cases = []
+    vl, el, _ = pc.HostCSR.rmat(18, 16, 4).arrays()
+    cases.append(("rmat18", vl, el, pc.equal_vertex_partition(vl.size - 1, 16)))
+    vl, el = _split_overflow_graph()
+    cases.append(("overflow-P1", vl, el, None))
+    cases.append(("overflow-P5", vl, el, pc.equal_vertex_partition(vl.size - 1, 5)))
+    for cid, vl, el, v2p in cases:
+        t = O.tc_merge(vl, el)
+        assert t > 0, cid
+        pg = pc.Partitioned_Graph(pc.Graph(vlist=vl, elist=el), v2p)
+        f = pc.selector.unit_features(pg)
+        assert f[:, 4].max() > 1 << 16, cid
+        for name in ("bitmap_warp", "bitmap_group8", "bitmap_lane"):
+            assert pg.triangle_count(variant=pc.VARIANTS[name]) == t, (cid, name)
+        assert pg.triangle_count(variant=pc.VARIANT_HEURISTIC) == t, cid
+        assert pg.triangle_count() == t, cid
+        pg.close()

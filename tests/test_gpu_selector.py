@@ -191,18 +191,20 @@ def test_insitu_collection_charges_every_unit(gpu, O):
     g.close()
 
 
-def test_learned_selector_gains_on_config5(gpu):
+def test_learned_selector_on_config5(gpu):
     """What the trained network gains over the method without it, on config 5
     (RMAT-25 ef16 seed 1, 2048 partitions).  The training data are in-situ
     unit costs the library measures on other graphs (RMAT-22 and RMAT-24, and
     two RMAT-25 graphs with other seeds); the plain heuristic is autotuned on
-    the same samples.  On this graph the plain rule sends every unit whose
-    largest pivot set exceeds the hash capacity to a bitmap kernel, whose
-    bitmaps then span hundreds of thousands of ids; the trained network finds
-    the hash kernel (with its merge fallback for the few large sets) several
-    times faster on those units.  Asserted: the leave-one-graph-out judge
-    accepts the model, the learned plan's measured counting time is at least
-    1.2x below the plain plan's, and both counts equal the pinned T."""
+    the same samples.  Before the bitmap kernels held high-id pivot sets as
+    split sets, the plain rule's bitmaps spanned hundreds of thousands of ids
+    on this graph and the network gained 1.33x by moving those units to the
+    hash kernel; with split sets the plain plan is within a few per cent of
+    the per-unit optimum, so the network has little left to gain.  Asserted:
+    both counts equal the pinned T, the learned plan is not slower than the
+    plain one beyond timing noise (the leave-one-graph-out judge keeps the
+    heuristic wherever the model does not beat it), and the plain plan is
+    within 10 % of the sum of the per-unit best in-situ costs on this graph."""
     import json
 
     from conftest import GOLDEN
@@ -221,7 +223,7 @@ def test_learned_selector_gains_on_config5(gpu):
         sel.autotune()
         sel.train(steps=1500, lr=3e-3, seed=7)
         margin, gain = sel.judge()
-        assert np.isfinite(margin) and gain > 1.0, (margin, gain)
+        assert gain >= 1.0, (margin, gain)
         want = json.loads((GOLDEN / "pinned_counts.json").read_text())["rmat25_ef16_s1"]["T"]
         g = pc.Graph.rmat_device(25, 16, 1)
         pg = pc.Partitioned_Graph(g, pc.equal_vertex_partition(g.get_vertex_num(), 2048))
@@ -234,9 +236,21 @@ def test_learned_selector_gains_on_config5(gpu):
                 assert c == want
                 times.append(st.kernel_ms)
             ms[name] = float(np.median(times))
+        assert ms["learned"] <= 1.05 * ms["plain"], ms
+        # in-situ cost of every variant on every unit of this graph: the plain
+        # plan's units against the best variant of each unit
+        n0 = sel.num_samples()
+        sel.collect_insitu(pg, repeats=1)
+        _, y, m = sel.samples()
+        cost = np.where(m[n0:].astype(bool), np.exp(y[n0:].astype(np.float64)), np.inf)
+        plan = sel.plan(pg, pc.VARIANT_HEURISTIC)
+        plan = plan[plan >= 0].astype(np.int64)
+        assert plan.size == cost.shape[0]
+        best = float(cost.min(axis=1).sum())
+        plain = float(cost[np.arange(plan.size), plan].sum())
+        assert plain <= 1.10 * best, (plain, best)
         pg.close()
         g.close()
-        assert ms["plain"] >= 1.2 * ms["learned"], ms
     finally:
         sel.clear()
         sel.set_heuristic(hp0)
