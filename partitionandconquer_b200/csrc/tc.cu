@@ -221,7 +221,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // at the 16-byte boundary at or below the span (up to 3 ids early) and may
 // end up to 3 ids past it, which the 64 ids of padding after the last row
 // keep inside the adjacency array.
-constexpr uint32_t kStageIds = 512;
+constexpr uint32_t kStageIds = 256;
 
 // Issues the copies of ids [r, r + k) of adj into stage; returns the offset
 // of id r inside it, or -1 when the span does not fit (it is then read from
@@ -641,7 +641,7 @@ static int matrix_pivot_block() {
 }
 
 // Matrix launch shape: warps per CTA (kMatrixWarps, or PC_MATRIX_WARPS=4) and
-// ids per span stage (kStageIds, or PC_MATRIX_STAGE_IDS=128|256|1024), read
+// ids per span stage (kStageIds, or PC_MATRIX_STAGE_IDS=128|512|1024), read
 // once from the environment; switches for measurements.
 static int matrix_env(const char* name, int dflt, std::initializer_list<int> allowed) {
     const char* e = getenv(name);
