@@ -238,9 +238,11 @@ __device__ __forceinline__ int stage_span(const int32_t* __restrict__ adj, uint6
 
 // Word form of a block whose last pivot b sits at position jl: ceil(b/128)
 // 16-byte words per row against ceil(jl/32) probe rounds.
-__device__ __forceinline__ bool matrix_words_win(int32_t b, uint32_t jl) {
+// With pshift = 1 a probe round counts twice: when S is read from global
+// memory, a probe round waits on the load of S[i] and then on the row word.
+__device__ __forceinline__ bool matrix_words_win(int32_t b, uint32_t jl, uint32_t pshift) {
     const uint32_t nv = ((((uint32_t)b + 31) >> 5) + 3) >> 2;
-    return ((nv + 31) >> 5) < ((jl + 31) >> 5);
+    return ((nv + 31) >> 5) < (((jl + 31) >> 5) << pshift);
 }
 
 // The pairs (b, c) of one in-neighbour c: S = N(c) & [0, min(hi, c)), pivots
@@ -258,12 +260,12 @@ template <int U>
 __device__ __forceinline__ unsigned long long matrix_block_pairs(const int32_t* S, uint32_t j0, uint32_t k,
                                                                  int32_t lo, uint32_t hstride,
                                                                  const uint32_t* __restrict__ H, uint32_t* Sb,
-                                                                 int lane) {
+                                                                 int lane, uint32_t pshift) {
     unsigned long long cnt = 0;
     bool want = false;
     for (uint32_t jb = j0 + (uint32_t)lane * U; jb < k; jb += 32u * U) {
         const uint32_t jl = min(jb + (uint32_t)U, k) - 1;
-        want |= matrix_words_win(S[jl], jl);
+        want |= matrix_words_win(S[jl], jl, pshift);
     }
     const bool words = __any_sync(0xffffffffu, want);
     if (words) {
@@ -283,7 +285,7 @@ __device__ __forceinline__ unsigned long long matrix_block_pairs(const int32_t* 
             const int32_t b = (uint32_t)u < ju ? S[jb + u] : bl;
             h[u] = H + (uint64_t)(b - lo) * hstride;
         }
-        if (words && matrix_words_win(bl, jl)) {
+        if (words && matrix_words_win(bl, jl, pshift)) {
             const uint32_t nv = ((((uint32_t)bl + 31) >> 5) + 3) >> 2;
             for (uint32_t x = lane; x < nv; x += 32) {
                 const uint4 sv = Sb4[x];
@@ -343,7 +345,7 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
                                                                unsigned long long* __restrict__ next,
                                                                unsigned long long* __restrict__ total,
                                                                unsigned long long* __restrict__ unit_cost,
-                                                               int32_t unit, uint32_t svec) {
+                                                               int32_t unit, uint32_t svec, uint32_t gprobe) {
     extern __shared__ uint4 msm4[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t nwarps = blockDim.x >> 5;  // kMatrixWarps or fewer
@@ -365,7 +367,7 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
         r = __shfl_sync(0xffffffffu, r, 0);
         klo = __shfl_sync(0xffffffffu, klo, 0);
         khi = __shfl_sync(0xffffffffu, khi, 0);
-        if (khi > klo) cnt += matrix_block_pairs<U>(adj + r, klo, khi, lo, hstride, H, Sb, lane);
+        if (khi > klo) cnt += matrix_block_pairs<U>(adj + r, klo, khi, lo, hstride, H, Sb, lane, gprobe);
     }
     for (;;) {  // phase 2: 32 in-neighbours per grab, spans staged two deep
         unsigned long long q = 0;
@@ -399,7 +401,7 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
             const uint32_t k = __shfl_sync(0xffffffffu, khi, src);
             const int32_t* S = shift >= 0 ? reinterpret_cast<const int32_t*>(stage + buf * svec) + shift
                                           : adj + rs;
-            cnt += matrix_block_pairs<U>(S, j0, k, lo, hstride, H, Sb, lane);
+            cnt += matrix_block_pairs<U>(S, j0, k, lo, hstride, H, Sb, lane, shift >= 0 ? 0u : gprobe);
             __syncwarp();  // the buffer just read is the next stage's target
             if (nxt < 0) break;
             src = nxt;
@@ -514,10 +516,16 @@ static pc_status launch_bitmap_kgv(const BitmapLaunch& L) {
     return PC_OK;
 }
 
-// Split-set launches (count mode): sets of kSplitWords + kHashSlots words
-// (10 KB), so bitmap_shape gives K = 2 for every such launch.
+// Split-set launches: sets of kSplitWords + kHashSlots words (10 KB); K = 2
+// in the count mode (16 sets per SM), K = 4 in the per-vertex mode, whose
+// 32 KB hub histogram per CTA would leave one CTA of 8 sets per SM.
 static pc_status launch_bitmap_split(int K, int G, const BitmapLaunch& L) {
-    if (K != 2 || L.tri || L.ecnt) return fail(PC_ERR_UNSUPPORTED, "split pivot sets: unexpected launch shape");
+    if (L.ecnt || (L.tri ? K != 4 : K != 2)) return fail(PC_ERR_UNSUPPORTED, "split pivot sets: unexpected launch shape");
+    if (L.tri) {
+        if (G == 32) return launch_bitmap_kgv<4, 32, true, false, true>(L);
+        if (G == 8) return launch_bitmap_kgv<4, 8, true, false, true>(L);
+        return launch_bitmap_kgv<4, 1, true, false, true>(L);
+    }
     if (G == 32) return launch_bitmap_kgv<2, 32, false, false, true>(L);
     if (G == 8) return launch_bitmap_kgv<2, 8, false, false, true>(L);
     return launch_bitmap_kgv<2, 1, false, false, true>(L);
@@ -620,8 +628,8 @@ static uint32_t matrix_stride(int64_t hi) { return (uint32_t)((((hi + 31) / 32) 
 static uint64_t matrix_bytes(int64_t lo, int64_t hi) { return (uint64_t)(hi - lo) * matrix_stride(hi) * 4; }
 
 // Bitmap units whose pivot ids reach kSplitLo or more run with SplitSets in
-// the count mode, unless PC_BITMAP_SPLIT=0 is in the environment (read once;
-// a switch for measurements).
+// the count and per-vertex modes, unless PC_BITMAP_SPLIT=0 is in the
+// environment (read once; a switch for measurements).
 static bool bitmap_split_enabled() {
     static const bool on = [] {
         const char* e = getenv("PC_BITMAP_SPLIT");
@@ -655,6 +663,12 @@ static int matrix_warps() {
     static const int w = matrix_env("PC_MATRIX_WARPS", kMatrixWarps, {4, 8});
     return w;
 }
+// 1 with PC_MATRIX_GLOBAL_PROBE=2: a probe round over a span read from
+// global memory counts as two when the block form is chosen (measurements).
+static uint32_t matrix_global_probe_shift() {
+    static const uint32_t v = matrix_env("PC_MATRIX_GLOBAL_PROBE", 1, {1, 2}) == 2 ? 1u : 0u;
+    return v;
+}
 static uint32_t matrix_stage_vec() {
     static const uint32_t v = (uint32_t)matrix_env("PC_MATRIX_STAGE_IDS", (int)kStageIds, {128, 256, 512, 1024}) / 4 + 1;
     return v;
@@ -672,7 +686,7 @@ static pc_status launch_matrix(pc_pgraph* pg, int64_t lo, int64_t hi, uint32_t h
     PC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_matrix<U>, warps * 32, smem));
     k_tc_matrix<U><<<(unsigned)(sms * std::max(1, per_sm)), warps * 32, smem, s>>>(
         pg->off, pg->adj, pg->dplus.as<uint32_t>(), (int32_t)lo, (int32_t)hi, pg->g->n, hstride, H, d_next, d_total,
-        d_cost, unit, svec);
+        d_cost, unit, svec, matrix_global_probe_shift());
     PC_LAUNCHED();
     return PC_OK;
 }
@@ -734,7 +748,11 @@ static pc_status run_group(pc_pgraph* pg, const LaunchGroup& gr, unsigned long l
     int64_t* d_pref = nullptr;
     PC_TRY(upload(pg, gr.ranges.data(), gr.ranges.size(), &d_ranges));
     PC_TRY(upload(pg, pref.data(), nr + 1, &d_pref));
-    const BitmapShape sh = bitmap_shape((gr.split ? kSplitWords + (uint32_t)kHashSlots : gr.words) * 32u);
+    BitmapShape sh = bitmap_shape((gr.split ? kSplitWords + (uint32_t)kHashSlots : gr.words) * 32u);
+    if (gr.split && d_tri) {
+        sh.K = 4;
+        sh.smem = (size_t)(16 / sh.K) * (kSplitWords + kHashSlots) * 4;
+    }
     const uint32_t chunk = is_bitmap(v) ? 256u * (uint32_t)sh.K : (uint32_t)kChunkWarp;
     uint32_t* d_cnt = pg->scratch.take<uint32_t>(npos + 1);
     uint32_t* d_start = pg->scratch.take<uint32_t>(npos + 1);
@@ -841,10 +859,10 @@ static pc_status tc_execute(pc_pgraph* pg, const std::vector<int8_t>& assign, ui
     const size_t U = lo.size();
     // Bitmap units are grouped by their bitmap size rounded up to a power of
     // two, so the hub units (small ids) get small sets and more CTAs per SM;
-    // in the count mode, units with pivot ids past kSplitLo share one group of
-    // fixed-size SplitSets (class kClasses).
+    // in the count and per-vertex modes, units with pivot ids past kSplitLo
+    // share one group of fixed-size SplitSets (class kClasses).
     constexpr int kClasses = 16;
-    const bool split_ok = bitmap_split_enabled() && !d_tri && !d_ecnt;
+    const bool split_ok = bitmap_split_enabled() && !d_ecnt;
     std::vector<LaunchGroup> groups(PC_NUM_VARIANTS * (kClasses + 1));
     std::vector<int> group_of(U, -1);
     for (size_t u = 0; u < U; ++u) {

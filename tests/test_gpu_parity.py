@@ -348,11 +348,11 @@ def test_matrix_form_on_hub_units(gpu, O, scale, P):
 
 
 def test_bitmap_kernels_every_set_shape(gpu, O):
-    """Forced bitmap variants on RMAT-20 with 64 partitions.  In the count
-    mode units with pivot ids past 2^16 hold split sets (K = 2); in the
-    per-vertex mode (LCC) pivot ids up to 2^20 make the kernels share one
-    plain bitmap among K = 1, 2, 4, 8 and 16 warps (named barriers) across the
-    units.  Counts and LCC must equal the oracle's."""
+    """Forced bitmap variants on RMAT-20 with 64 partitions: units with pivot
+    ids past 2^16 hold split sets (K = 2 in the count mode, K = 4 in the
+    per-vertex mode of LCC).  Counts and LCC must equal the oracle's.  The
+    per-edge mode's plain bitmaps of every size are covered by
+    test_per_edge_mode_every_set_shape."""
     pc = gpu
     h = pc.HostCSR.rmat(20, 16, 5)
     vl, el, _ = h.arrays()
@@ -365,9 +365,8 @@ def test_bitmap_kernels_every_set_shape(gpu, O):
     f = pc.selector.unit_features(pg)
     assert f[:, 1].sum() == el.size // 2  # every in-edge belongs to one unit
     assert (f[:, 0].sum(), f[:, 4].max()) == (n, n)
-    # per-vertex mode (LCC) keeps the plain bitmaps of every size: a plan with
-    # the 8-lane bitmap kernel wherever it is feasible shares one set among
-    # K = 1 ... 16 warps across the units
+    # per-vertex mode (LCC) under a plan with the 8-lane bitmap kernel wherever
+    # it is feasible: plain bitmaps below id 2^16, split sets above
     saved = pc.selector.get_heuristic()
     try:
         pc.selector.set_heuristic([0.0, 1e9, 0.0, 1e9])
@@ -429,4 +428,43 @@ def test_split_pivot_sets(gpu, O):
             assert pg.triangle_count(variant=pc.VARIANTS[name]) == t, (cid, name)
         assert pg.triangle_count(variant=pc.VARIANT_HEURISTIC) == t, cid
         assert pg.triangle_count() == t, cid
+        # per-vertex mode (LCC) with split sets, under a bitmap plan
+        saved = pc.selector.get_heuristic()
+        try:
+            pc.selector.set_heuristic([0.0, 1e9, 0.0, 1e9])
+            lcc = pg.solve_lcc_merge()
+        finally:
+            pc.selector.set_heuristic(saved)
+        want = O.lcc(vl, el)
+        np.testing.assert_array_equal(np.isnan(lcc), np.isnan(want), err_msg=cid)
+        np.testing.assert_array_equal(lcc, want, err_msg=cid)
         pg.close()
+
+
+def test_per_edge_mode_every_set_shape(gpu, O):
+    """All-edge Jaccard (per-edge mode, which keeps plain bitmaps for the ranks
+    of its hits) under a plan with the 8-lane bitmap kernel wherever it is
+    feasible, on a Chung-Lu graph with 2^20 vertices (exponent 2.1, 2^22
+    edges, 4.9 M triangles) and 16 partitions: pivot ids up to 2^20 make the
+    kernels share one bitmap among K = 1, 2, 4, 8 and 16 warps; LCC under the
+    same plan uses split sets past 2^16.  Both equal the oracle's."""
+    pc = gpu
+    vl, el, _ = pc.HostCSR.chung_lu(20, 1 << 22, 2.1, 1 << 12, 3).arrays()
+    n = vl.size - 1
+    pg = pc.Partitioned_Graph(pc.Graph(vlist=vl, elist=el), pc.equal_vertex_partition(n, 16))
+    assert pc.selector.unit_features(pg)[:, 4].max() > 1 << 19
+    saved = pc.selector.get_heuristic()
+    try:
+        pc.selector.set_heuristic([0.0, 1e9, 0.0, 1e9])
+        jac = pg.jaccard_edges()
+        lcc = pg.solve_lcc_merge()
+        c, st = pg.triangle_count(variant=pc.VARIANT_HEURISTIC, stats=True)
+    finally:
+        pc.selector.set_heuristic(saved)
+    assert st.variant_hist[pc.VARIANTS["bitmap_group8"]] > 0
+    assert c == O.tc_merge(vl, el)
+    np.testing.assert_array_equal(jac, O.jaccard_edges(vl, el))
+    want = O.lcc(vl, el)
+    np.testing.assert_array_equal(np.isnan(lcc), np.isnan(want))
+    np.testing.assert_array_equal(lcc, want)
+    pg.close()
