@@ -238,11 +238,9 @@ __device__ __forceinline__ int stage_span(const int32_t* __restrict__ adj, uint6
 
 // Word form of a block whose last pivot b sits at position jl: ceil(b/128)
 // 16-byte words per row against ceil(jl/32) probe rounds.
-// With pshift = 1 a probe round counts twice: when S is read from global
-// memory, a probe round waits on the load of S[i] and then on the row word.
-__device__ __forceinline__ bool matrix_words_win(int32_t b, uint32_t jl, uint32_t pshift) {
+__device__ __forceinline__ bool matrix_words_win(int32_t b, uint32_t jl) {
     const uint32_t nv = ((((uint32_t)b + 31) >> 5) + 3) >> 2;
-    return ((nv + 31) >> 5) < (((jl + 31) >> 5) << pshift);
+    return ((nv + 31) >> 5) < ((jl + 31) >> 5);
 }
 
 // The pairs (b, c) of one in-neighbour c: S = N(c) & [0, min(hi, c)), pivots
@@ -260,12 +258,12 @@ template <int U>
 __device__ __forceinline__ unsigned long long matrix_block_pairs(const int32_t* S, uint32_t j0, uint32_t k,
                                                                  int32_t lo, uint32_t hstride,
                                                                  const uint32_t* __restrict__ H, uint32_t* Sb,
-                                                                 int lane, uint32_t pshift) {
+                                                                 int lane) {
     unsigned long long cnt = 0;
     bool want = false;
     for (uint32_t jb = j0 + (uint32_t)lane * U; jb < k; jb += 32u * U) {
         const uint32_t jl = min(jb + (uint32_t)U, k) - 1;
-        want |= matrix_words_win(S[jl], jl, pshift);
+        want |= matrix_words_win(S[jl], jl);
     }
     const bool words = __any_sync(0xffffffffu, want);
     if (words) {
@@ -285,7 +283,7 @@ __device__ __forceinline__ unsigned long long matrix_block_pairs(const int32_t* 
             const int32_t b = (uint32_t)u < ju ? S[jb + u] : bl;
             h[u] = H + (uint64_t)(b - lo) * hstride;
         }
-        if (words && matrix_words_win(bl, jl, pshift)) {
+        if (words && matrix_words_win(bl, jl)) {
             const uint32_t nv = ((((uint32_t)bl + 31) >> 5) + 3) >> 2;
             for (uint32_t x = lane; x < nv; x += 32) {
                 const uint4 sv = Sb4[x];
@@ -345,7 +343,7 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
                                                                unsigned long long* __restrict__ next,
                                                                unsigned long long* __restrict__ total,
                                                                unsigned long long* __restrict__ unit_cost,
-                                                               int32_t unit, uint32_t svec, uint32_t gprobe) {
+                                                               int32_t unit, uint32_t svec) {
     extern __shared__ uint4 msm4[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t nwarps = blockDim.x >> 5;  // kMatrixWarps or fewer
@@ -367,7 +365,7 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
         r = __shfl_sync(0xffffffffu, r, 0);
         klo = __shfl_sync(0xffffffffu, klo, 0);
         khi = __shfl_sync(0xffffffffu, khi, 0);
-        if (khi > klo) cnt += matrix_block_pairs<U>(adj + r, klo, khi, lo, hstride, H, Sb, lane, gprobe);
+        if (khi > klo) cnt += matrix_block_pairs<U>(adj + r, klo, khi, lo, hstride, H, Sb, lane);
     }
     for (;;) {  // phase 2: 32 in-neighbours per grab, spans staged two deep
         unsigned long long q = 0;
@@ -401,7 +399,7 @@ __global__ void __launch_bounds__(kMatrixWarps * 32) k_tc_matrix(const uint64_t*
             const uint32_t k = __shfl_sync(0xffffffffu, khi, src);
             const int32_t* S = shift >= 0 ? reinterpret_cast<const int32_t*>(stage + buf * svec) + shift
                                           : adj + rs;
-            cnt += matrix_block_pairs<U>(S, j0, k, lo, hstride, H, Sb, lane, shift >= 0 ? 0u : gprobe);
+            cnt += matrix_block_pairs<U>(S, j0, k, lo, hstride, H, Sb, lane);
             __syncwarp();  // the buffer just read is the next stage's target
             if (nxt < 0) break;
             src = nxt;
@@ -663,12 +661,6 @@ static int matrix_warps() {
     static const int w = matrix_env("PC_MATRIX_WARPS", kMatrixWarps, {4, 8});
     return w;
 }
-// 1 with PC_MATRIX_GLOBAL_PROBE=2: a probe round over a span read from
-// global memory counts as two when the block form is chosen (measurements).
-static uint32_t matrix_global_probe_shift() {
-    static const uint32_t v = matrix_env("PC_MATRIX_GLOBAL_PROBE", 1, {1, 2}) == 2 ? 1u : 0u;
-    return v;
-}
 static uint32_t matrix_stage_vec() {
     static const uint32_t v = (uint32_t)matrix_env("PC_MATRIX_STAGE_IDS", (int)kStageIds, {128, 256, 512, 1024}) / 4 + 1;
     return v;
@@ -686,7 +678,7 @@ static pc_status launch_matrix(pc_pgraph* pg, int64_t lo, int64_t hi, uint32_t h
     PC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_matrix<U>, warps * 32, smem));
     k_tc_matrix<U><<<(unsigned)(sms * std::max(1, per_sm)), warps * 32, smem, s>>>(
         pg->off, pg->adj, pg->dplus.as<uint32_t>(), (int32_t)lo, (int32_t)hi, pg->g->n, hstride, H, d_next, d_total,
-        d_cost, unit, svec, matrix_global_probe_shift());
+        d_cost, unit, svec);
     PC_LAUNCHED();
     return PC_OK;
 }
