@@ -382,7 +382,7 @@ def train_selector(pc, args):
     as config 3's), all with other seeds than the measured graphs; each is
     partitioned into 16 K-vertex units like the measured graphs.  The
     heuristic is autotuned on the samples (its best threshold sets by in-situ
-    unit costs, then timed as whole plans on two of the training graphs), then
+    unit costs, then timed as whole plans on three of the training graphs), then
     the MLP is trained on the GPU (each unit weighted by its time) with its
     judge margin chosen by leave-one-graph-out validation."""
     sel = pc.selector
@@ -396,7 +396,7 @@ def train_selector(pc, args):
               lambda: pc.Graph.er_device(s - 2, 1 << (s + 2), args.seed + 2),
               lambda: pc.Graph(host=pc.HostCSR.chung_lu(s - 2, 1 << (s + 2), 2.1, 1 << (s - 6), args.seed + 3)),
               lambda: pc.Graph(host=pc.HostCSR.chung_lu(s, 1 << (s + 4), 2.1, 1 << (s - 4), args.seed + 6))]
-    keep = {2, 3}  # RMAT-(s+2) and the first RMAT-25 verify the autotuner's candidates
+    keep = {2, 3, 7}  # RMAT-(s+2), the first RMAT-25 and Chung-Lu-(s) verify the autotuner's candidates
     kept = []
     for i, make in enumerate(graphs):
         g = make()
@@ -416,8 +416,9 @@ def train_selector(pc, args):
     margin, gain = sel.judge()
     return {"samples": sel.num_samples(), "train_loss": loss, "heuristic_params": tuned.tolist(),
             "autotune": f"8 best threshold sets by in-situ unit costs, and the defaults, timed on RMAT-{s + 2} "
-                        f"(seed {args.seed + 5}) and RMAT-25 (seed {args.seed + 1}): {round(verify_ms, 2)} ms summed "
-                        "for the kept set",
+                        f"(seed {args.seed + 5}), RMAT-25 (seed {args.seed + 1}) and Chung-Lu at 2^{s} (mean degree "
+                        f"32); kept: the lowest sum of per-graph times relative to each graph's fastest set "
+                        f"({round(verify_ms, 2)} ms summed)",
             "judge_margin": None if not np.isfinite(margin) else round(float(np.exp(margin)), 4),
             "heldout_gain_vs_plain": round(gain, 4),
             "training_graphs": f"RMAT-{s - 2}/{s}/{s + 2} and RMAT-25 x2 (seeds {args.seed + 4}, {args.seed + 1}, "

@@ -367,8 +367,9 @@ pc_status pc_selector_autotune(double* tuned /* 4 */);
 /* Two-stage autotuning: the k best threshold sets by the same grid search on
  * the collected samples (distinct plans only), plus the thresholds in force,
  * are each applied and timed on the npg graph views (the heuristic plan's
- * counting time, median of `repeats` after one warm-up call); the set with
- * the lowest summed time is kept and returned with that time.  The views
+ * counting time, median of `repeats` after one warm-up call).  Every view
+ * weighs alike: the kept set has the lowest sum over views of its time over
+ * the fastest set's time there; measured_ms is its summed time.  The views
  * should be graphs other than the ones the plan is measured on. */
 pc_status pc_selector_autotune_measured(pc_pgraph* const* pgs, int32_t npg, int32_t k, int32_t repeats,
                                         double* tuned /* 4 */, double* measured_ms);

@@ -1008,11 +1008,10 @@ pc_status pc_selector_autotune_measured(pc_pgraph* const* pgs, int32_t npg, int3
     // the thresholds in force before tuning compete too
     cand.push_back(heuristic_params());
     const HeuristicParams before = heuristic_params();
-    double best_ms = INFINITY;
-    size_t best = 0;
+    // ms[c * npg + i]: median counting time of candidate c on view i
+    std::vector<double> ms(cand.size() * (size_t)npg, 0.0);
     for (size_t c = 0; c < cand.size(); ++c) {
         set_heuristic_params(cand[c]);
-        double sum = 0;
         for (int32_t i = 0; i < npg; ++i) {
             PC_TRY(use_device(pgs[i]->g));
             std::vector<double> t;
@@ -1033,16 +1032,31 @@ pc_status pc_selector_autotune_measured(pc_pgraph* const* pgs, int32_t npg, int3
                 }
             }
             std::sort(t.begin(), t.end());
-            sum += t[t.size() / 2];
+            ms[c * npg + i] = t[t.size() / 2];
         }
-        if (sum < best_ms) {
-            best_ms = sum;
+    }
+    // each view weighs alike: a candidate scores the sum over views of its time
+    // over the fastest candidate's time on that view
+    std::vector<double> fastest(npg, INFINITY);
+    for (size_t c = 0; c < cand.size(); ++c)
+        for (int32_t i = 0; i < npg; ++i) fastest[i] = std::min(fastest[i], ms[c * npg + i]);
+    double best_score = INFINITY;
+    size_t best = 0;
+    for (size_t c = 0; c < cand.size(); ++c) {
+        double score = 0;
+        for (int32_t i = 0; i < npg; ++i) score += ms[c * npg + i] / std::max(fastest[i], 1e-9);
+        if (score < best_score) {
+            best_score = score;
             best = c;
         }
     }
     set_heuristic_params(cand[best]);
     if (tuned) params_out(cand[best], tuned);
-    if (measured_ms) *measured_ms = best_ms;
+    if (measured_ms) {
+        double sum = 0;
+        for (int32_t i = 0; i < npg; ++i) sum += ms[best * npg + i];
+        *measured_ms = sum;
+    }
     return PC_OK;
 }
 

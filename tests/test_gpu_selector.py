@@ -254,3 +254,32 @@ def test_learned_selector_on_config5(gpu):
     finally:
         sel.clear()
         sel.set_heuristic(hp0)
+
+
+def test_measured_autotune_keeps_a_timed_threshold_set(gpu, O):
+    """pc_selector_autotune_measured: the best threshold sets by the collected
+    in-situ costs, and the thresholds in force, are timed as whole plans on
+    the given views; the kept set is the one in force afterwards, its summed
+    time is positive, and counts under it stay exact."""
+    pc = gpu
+    sel = pc.selector
+    hp0 = sel.get_heuristic()
+    sel.clear()
+    try:
+        views = []
+        for scale, seed in ((16, 3), (17, 4)):
+            vl, el, _ = pc.HostCSR.rmat(scale, 16, seed).arrays()
+            g = pc.Graph(vlist=vl, elist=el)
+            pg = pc.Partitioned_Graph(g, pc.equal_vertex_partition(vl.size - 1, 16))
+            assert sel.collect_insitu(pg, repeats=1) > 0
+            views.append((g, pg, O.tc_merge(vl, el)))
+        tuned, ms = sel.autotune(verify=[pg for _, pg, _ in views], k=4, repeats=2)
+        assert ms > 0 and tuned.shape == (4,)
+        assert np.array_equal(sel.get_heuristic(), tuned)
+        for g, pg, t in views:
+            assert pg.triangle_count(variant=pc.VARIANT_HEURISTIC) == t
+            pg.close()
+            g.close()
+    finally:
+        sel.clear()
+        sel.set_heuristic(hp0)
