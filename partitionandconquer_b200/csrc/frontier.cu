@@ -504,7 +504,7 @@ __device__ __forceinline__ KState load_state(const KState* p) {
 __global__ void __launch_bounds__(kThreads) k_kcore_persistent(
     const uint64_t* __restrict__ off, const int32_t* __restrict__ adj, uint64_t n, int32_t* deg, int32_t* core,
     int32_t* rem0, int32_t* rem1, int32_t* f0, int32_t* f1, int32_t* hq0, int32_t* hq1, KState* S,
-    GridBarrier* gb, uint64_t max_steps, uint64_t limit_ns, uint64_t* steps_done) {
+    GridBarrier* gb, uint64_t max_steps, uint64_t limit_ns, uint64_t* steps_done, uint32_t local_edges) {
     // decrements of the lowest ids (the hubs, once ids are degree-ordered)
     // are gathered per CTA in shared memory and applied once per step
     __shared__ int32_t s_dec[kKcoreHubs];
@@ -634,7 +634,7 @@ __global__ void __launch_bounds__(kThreads) k_kcore_persistent(
                     }
                     if (cnt == 0) break;
                 }
-                if (s_lqe[rd] > kLocalEdges) {
+                if (s_lqe[rd] > local_edges) {
                     // too much for one CTA: the next step shares it among all
                     const uint32_t cpad = (cnt + 31) & ~31u;
                     for (uint32_t i = threadIdx.x; i < cpad; i += blockDim.x)
@@ -1253,6 +1253,18 @@ pc_status pc_selftest_grid_barrier(int32_t device, int32_t rounds, int32_t absen
     return PC_OK;
 }
 
+// Row entries of a CTA's local queue above which the queue goes to the next
+// step's frontier (shared by every CTA): kLocalEdges, or PC_KCORE_LOCAL_EDGES
+// from the environment (read once; a switch for measurements).
+static uint32_t kcore_local_edges() {
+    static const uint32_t v = [] {
+        const char* e = getenv("PC_KCORE_LOCAL_EDGES");
+        const long x = e ? atol(e) : (long)kLocalEdges;
+        return (uint32_t)std::max(64L, std::min(x, 1L << 20));
+    }();
+    return v;
+}
+
 pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
     clear_error();
     if (!pg || !core_host) return fail(PC_ERR_INVALID_INPUT, "null argument");
@@ -1305,9 +1317,10 @@ pc_status pc_kcore(pc_pgraph* pg, int32_t* core_host, int32_t* largest) {
     const uint64_t* off = pg->off;
     const int32_t* adj = pg->adj;
     uint64_t nn = n;
+    uint32_t local_edges = kcore_local_edges();
     void* args[] = {(void*)&off,  (void*)&adj, (void*)&nn, (void*)&deg, (void*)&core, (void*)&rem0,
                     (void*)&rem1, (void*)&f0,  (void*)&f1, (void*)&hq0, (void*)&hq1,  (void*)&S,
-                    (void*)&gb,   (void*)&max_steps, (void*)&limit_ns, (void*)&d_steps};
+                    (void*)&gb,   (void*)&max_steps, (void*)&limit_ns, (void*)&d_steps, (void*)&local_edges};
     PC_CUDA(cudaLaunchCooperativeKernel((const void*)k_kcore_persistent, dim3(grid), dim3(kThreads), args, 0, s));
     PC_LAUNCHED();
     k_kcore_finish<<<nb, kThreads, 0, s>>>(core, n, d_top);

@@ -420,8 +420,15 @@ constexpr uint32_t kBitmapCapBits = 1u << 20;  // 128 KB of shared memory
 
 static bool bitmap_feasible(const float* f) { return f[4] <= (float)kBitmapCapBits; }
 // The in-neighbour-major form needs the unit's pivots to be the id range
-// [lo, hi) (contiguous partitions; tc_assign checks that) with hi <= 2^16.
-static bool matrix_feasible(const float* f) { return f[4] <= (float)kMatrixMaxId; }
+// [lo, hi) (contiguous partitions; tc_assign checks that) with hi <= 2^16,
+// and its resident rows to fit L2 (126 MB on B200): rows that spill re-read
+// DRAM on every probe, which is what the form exists to avoid (RMAT-24's
+// fourth hub unit, 128 MB of rows, cost 4 ms more than the bitmap kernel).
+constexpr double kMatrixRowsCap = 100.0 * (1 << 20);
+static bool matrix_feasible(const float* f) {
+    const double words = (double)((((uint64_t)f[4] + 31) / 32 + 3) & ~(uint64_t)3);
+    return f[4] <= (float)kMatrixMaxId && (double)f[0] * words * 4.0 <= kMatrixRowsCap;
+}
 
 // Plain autotuned heuristic.  Thresholds come from heuristic_params(), which
 // the autotuner (pc_selector_autotune) may replace.
@@ -987,7 +994,7 @@ pc_status tc_assign(pc_pgraph* pg, int32_t variant, const std::vector<float>& fe
             if (f[1] <= 0 || f[2] <= 0) continue;
             if (!variant_feasible(variant, f))
                 return fail(PC_ERR_UNSUPPORTED, variant == PC_VARIANT_MATRIX
-                                                    ? "forced matrix variant: a pivot id is 2^16 or above"
+                                                    ? "forced matrix variant: a pivot id is 2^16 or above, or a unit's rows exceed 100 MB"
                                                     : "forced bitmap variant: a pivot id exceeds the shared-memory "
                                                       "bitmap capacity");
             (*assign)[u] = (int8_t)variant;

@@ -304,11 +304,12 @@ def test_config1_rmat16(gpu, O):
     assert int(np.isnan(lcc).sum()) == s["lcc_nan"]
 
 
-@pytest.mark.parametrize("scale,P", [(16, 4), (19, 16)])
+@pytest.mark.parametrize("scale,P", [(16, 8), (19, 16)])
 def test_matrix_form_on_hub_units(gpu, O, scale, P):
     """The in-neighbour-major form (resident pivot bitmap rows, word-AND and
-    bit probes) on every unit whose ids are below 2^16, the other units by
-    the usual kernels: exact counts, forced where every unit qualifies."""
+    bit probes) on every unit whose ids are below 2^16 and whose rows fit
+    100 MB, the other units by the usual kernels: exact counts, forced where
+    every unit qualifies."""
     pc = gpu
     sel = pc.selector
     vl, el, _ = pc.HostCSR.rmat(scale, 16, 3).arrays()
