@@ -17,6 +17,8 @@
 //
 // Pivot sets in shared memory:
 //  * bitmap (CTA-wide): bit a set for a in N+(b), needs b <= capacity;
+//  * split (CTA-wide): a bitmap of the ids below 2^16 and a hash of the rest
+//    (SplitSet), for pivots past 2^16 in the count and per-vertex modes;
 //  * hash (warp-private): open addressing, <= 256 keys in 512 slots;
 //  * none: threshold merge (the reference's primitive) or binary search.
 #pragma once
@@ -92,26 +94,6 @@ struct SplitSet {
         return 0u;
     }
 };
-
-// Group-of-G scan of the prefix N(c) & [0, b): the G lanes of a group read G
-// consecutive ids per step (coalesced) and test them against the pivot set.
-// The scan stops at the first id >= b (rows are sorted) and never reads more
-// than lim = dplus[c] ids, so it stays inside row c.
-template <int G, class Test>
-__device__ __forceinline__ uint32_t scan_prefix(const int32_t* __restrict__ row, uint32_t lim, int32_t b, int gl,
-                                                unsigned gmask, Test test) {
-    uint32_t hits = 0;
-    for (uint32_t i = 0; i < lim; i += G) {
-        const uint32_t k = i + gl;
-        const int32_t a = k < lim ? __ldg(row + k) : 0x7fffffff;
-        if (a < b) hits += test(a);
-        int32_t last;
-        if constexpr (G == 1) last = a;
-        else last = __shfl_sync(gmask, a, G - 1, G);
-        if (last >= b) break;
-    }
-    return hits;
-}
 
 // Named barrier over `nthreads` threads of one warp group (ids 1..15; id 0
 // is __syncthreads).
